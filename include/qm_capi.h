@@ -1,0 +1,228 @@
+/*
+ * C-ABI of the B200-native per-keyframe depth pipeline (libqm_b200.so).
+ *
+ * Drop-in boundary for QuadtreeMapping's quadmap::Depthmap
+ * (include/quadmap/depthmap.h:31-89 of open_quadtree_mapping) and for the
+ * device stages behind it (SeedMatrix::extract_depth and fuse_output_depth,
+ * src/seed_matrix.cu:448-597).  Plain C: pointers, sizes and status codes;
+ * nothing throws across this boundary and no C++ or framework type appears
+ * in a signature.  include/qm_depthmap.hpp wraps it in the reference's C++
+ * class API.
+ *
+ * Conventions
+ *  - Every function returns a qm_status; qm_last_error() returns a
+ *    thread-local message for the last failure on the calling thread.
+ *  - Images are 8-bit grayscale, row pitch in BYTES.  Float maps are
+ *    row-major with a pitch in ELEMENTS where one is taken.
+ *  - Poses are 3x4 row-major float rigid transforms [R | t] as the
+ *    reference's SE3<float> stores them (se3.cuh:174, data(r, c) =
+ *    data[4r + c]); T_a_b maps points from frame b into frame a.
+ *  - Stage entry points take DEVICE pointers and a cudaStream_t passed as
+ *    void* (NULL = legacy default stream) and are asynchronous on it.
+ *    Facade and batch entry points take HOST buffers and are synchronous.
+ *  - Invalid fused depth is -1 (depth_fusion.cu:207-210).
+ */
+#ifndef QM_CAPI_H
+#define QM_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum qm_status {
+  QM_OK = 0,
+  QM_ERR_INVALID_ARG = 1, /* bad size, pointer, parameter */
+  QM_ERR_CUDA = 2,        /* a CUDA runtime call or kernel failed */
+  QM_ERR_NO_MEMORY = 3,   /* device or pinned allocation failed */
+  QM_ERR_STATE = 4,       /* call not valid in the object's current state */
+  QM_ERR_TIMEOUT = 5,     /* a bounded device wait gave up (error flag set) */
+  QM_ERR_WORKSPACE = 6    /* caller workspace too small */
+} qm_status;
+
+#define QM_MAX_BP_LEVELS 8
+#define QM_MAX_SLOTS 32     /* measurement slots per keyframe */
+#define QM_RING_CAPACITY 60 /* KEYFRAME_NUM, frameelement.cuh:9 */
+
+enum { QM_ARITH_REFERENCE = 0, QM_ARITH_IEEE = 1 };
+
+/* Algorithm parameters.  qm_params_default() gives the reference's compiled
+ * constants: DEPTH_NUM 64 (pixel_cost.cuh:4), MIN_INV_DEPTH 0.01 and
+ * STEP_INV_DEPTH (2.0-0.01)/63.0 (stereo_parameter.cuh:5-7), P1 0.003,
+ * P2 0.01 (bpextract.cu:222-223), 4 BP levels with {4,10,10,10} half-sweeps
+ * fine to coarse (bpextract.cu:41-45), quadtree max level 4, min level 2,
+ * threshold 10 (quadtree.cu:40,59,74), upsample sigma 400 and lambda 10
+ * (stereo_parameter.cuh upsample_sigma/upsample_lambda).
+ * arith: QM_ARITH_REFERENCE computes the projections and normalisations with
+ * the reference build's fast-math arithmetic (bit-exact costs and labels
+ * versus the reference kernels); QM_ARITH_IEEE uses IEEE-rounded operations
+ * (bit-exact versus the CPU oracle). */
+typedef struct qm_params {
+  int num_hyp;
+  double min_inv_depth;
+  double inv_depth_step;
+  float P1, P2;
+  int bp_levels;
+  int bp_iters[QM_MAX_BP_LEVELS]; /* fine -> coarse */
+  int qt_max_level;
+  int qt_min_level;
+  float qt_threshold;
+  double up_sigma;
+  double up_lambda;
+  int arith;
+} qm_params;
+
+typedef struct qm_camera {
+  float fx, fy, cx, cy; /* PinholeCamera order (pinhole_camera.cuh:42) */
+} qm_camera;
+
+/* ---------------------------------------------------------------- misc */
+void qm_params_default(qm_params *p);
+const char *qm_last_error(void);
+int qm_version(void); /* major*10000 + minor*100 + patch */
+
+/* ------------------------------------------------- Depthmap facade ----
+ * quadmap::Depthmap (depthmap.h:34-75, depthmap.cpp:19-68).  One camera
+ * stream: frame ring, frame-selection policy of SeedMatrix::add_frames
+ * (seed_matrix.cu:106-209), dense extraction and fusion.  The semi-dense
+ * tracker is not part of this library, so its projected depths are absent
+ * from the sparse input of the upsampler (the debug map holds the BP node
+ * depths only).  The image is expected undistorted (the reference's host
+ * cv::remap, seed_matrix.cu:85, stays with the caller). */
+typedef struct qm_depthmap qm_depthmap;
+
+/* Depthmap(width, height, fx, cx, fy, cy, remap_1, remap_2, semi2dense_ratio),
+ * depthmap.h:34-44 (note the fx, cx, fy, cy argument order). params NULL =
+ * reference defaults.  device = CUDA ordinal. */
+int qm_depthmap_create(qm_depthmap **out, int width, int height, float fx, float cx, float fy,
+                       float cy, int semi2dense_ratio, const qm_params *params, int device);
+int qm_depthmap_destroy(qm_depthmap *h);
+/* Depthmap::add_frames(img_curr, T_curr_world), depthmap.h:46-47.
+ * img: host u8 width x height, row pitch `stride` bytes.  T_curr_world:
+ * world->camera.  *has_result = 1 when a new depth map is available (the
+ * reference's boolean return). */
+int qm_depthmap_add_frame(qm_depthmap *h, const uint8_t *img, size_t stride,
+                          const float T_curr_world[12], int *has_result);
+/* getDepthmap (depthmap.h:49): fused depth, -1 where invalid. stride in elements. */
+int qm_depthmap_get_depth(qm_depthmap *h, float *out, size_t stride);
+/* getDebugmap (depthmap.h:50): the sparse depth handed to the upsampler. */
+int qm_depthmap_get_debug(qm_depthmap *h, float *out, size_t stride);
+/* getReferenceImage (depthmap.h:51): the image the last depth map belongs to. */
+int qm_depthmap_get_reference(qm_depthmap *h, uint8_t *out, size_t stride);
+/* getT_world_ref (depthmap.h:74). */
+int qm_depthmap_get_T_world_ref(qm_depthmap *h, float T[12]);
+/* getFx/Fy/Cx/Cy/Width/Height (depthmap.h:53-72). */
+int qm_depthmap_get_camera(qm_depthmap *h, qm_camera *cam, int *width, int *height);
+
+/* ------------------------------------------------------ batched streams
+ * N independent Depthmap streams of uneven size on one device.  One
+ * qm_batch_add_frames call runs the frame policy of every stream and then
+ * the dense pipeline of all streams that produce a depth map, one kernel
+ * launch per stage, replayed from a CUDA graph. */
+typedef struct qm_batch qm_batch;
+typedef struct qm_stream_desc {
+  int width, height;
+  qm_camera cam;
+  int num_hyp;          /* 0 = params->num_hyp */
+  int num_slots;        /* measurement slots (reference: 5) */
+  int semi2dense_ratio; /* seed_matrix.cuh:51 */
+} qm_stream_desc;
+
+int qm_batch_create(qm_batch **out, int num_streams, const qm_stream_desc *descs,
+                    const qm_params *params, int device);
+int qm_batch_destroy(qm_batch *b);
+/* imgs[i]: host u8 image of stream i (pitch strides[i] bytes), T_curr_world:
+ * num_streams*12 floats, has_result: num_streams ints (out). */
+int qm_batch_add_frames(qm_batch *b, const uint8_t *const *imgs, const size_t *strides,
+                        const float *T_curr_world, int *has_result);
+int qm_batch_get_depth(qm_batch *b, int stream, float *out, size_t stride);
+int qm_batch_get_debug(qm_batch *b, int stream, float *out, size_t stride);
+/* Re-runs the dense pipeline of every stream on the frames already resident
+ * on the device (no host transfers); used to time the device path alone. */
+int qm_batch_run_resident(qm_batch *b);
+/* Device pointer of stream i's fused depth map (row-major, dense). */
+int qm_batch_device_depth(qm_batch *b, int stream, const float **dev_ptr);
+/* 1 = replay captured CUDA graphs (default), 0 = launch stage by stage. */
+int qm_batch_set_graphs(qm_batch *b, int enable);
+/* Kernels launched by the last dense-pipeline run. */
+int qm_batch_last_launches(qm_batch *b, int *count);
+/* The cudaStream_t (as void*) every kernel of this batch is launched on;
+ * record timing events on it. */
+int qm_batch_stream(qm_batch *b, void **stream);
+/* Kernel kinds reported by qm_batch_profile, in this order. */
+#define QM_NUM_KERNEL_KINDS 12
+/* quadtree, cost, pyramid, message init/upsample, bp half-sweep, extraction,
+ * upsample weights, row solve, column solve, fuse transform, hole fill,
+ * fuse update.  Runs the resident pipeline once with eager launches, each
+ * bracketed by CUDA events; ms[k] and launches[k] receive the summed device
+ * time and the launch count of kind k.  No counterpart in the reference
+ * (its printf timers measure CPU clock time, seed_matrix.cu:482-546). */
+int qm_batch_profile(qm_batch *b, float ms[QM_NUM_KERNEL_KINDS],
+                     int launches[QM_NUM_KERNEL_KINDS]);
+
+/* ------------------------------------------- stage entry points --------
+ * One keyframe, device buffers, asynchronous on `stream`.  Stages that need
+ * scratch take a caller workspace whose size the *_workspace_size query
+ * returns (no allocation inside). */
+
+/* quadtree_image_kernal (quadtree.cu:17-77) as launched by
+ * SeedMatrix::extract_depth (seed_matrix.cu:469-480).
+ * levels: device u8 width*height (dense). */
+int qm_quadtree(const uint8_t *img, size_t img_pitch, int width, int height,
+                const qm_params *p, uint8_t *levels, void *stream);
+
+/* image_to_cost + normalize_the_cost (depth_extract.cu:135-244; launch
+ * seed_matrix.cu:486-524).  slots: HOST array of num_slots device image
+ * pointers (pitch slot_pitch bytes); T_slot_ref: HOST num_slots*12 floats
+ * (T_slot<-ref, the reference's FrameElement::transform).  Duplicated slots
+ * are allowed (the reference's slot->ring map repeats frame 0, see
+ * depth_extract.cu:153-166).  cost: device float (height/4)*(width/4)*num_hyp,
+ * cell-major with hypotheses contiguous (the PIXEL_COST layout,
+ * pixel_cost.cuh:11-37). */
+int qm_cost_volume(const uint8_t *ref, size_t ref_pitch, int width, int height,
+                   const qm_camera *cam, const uint8_t *levels, int num_slots,
+                   const uint8_t *const *slots, size_t slot_pitch, const float *T_slot_ref,
+                   const qm_params *p, float *cost, void *stream);
+
+/* bp_extract (bpextract.cu:37-167) with cost_distribute, upsample, bp and
+ * depth_extract (bpextract.cu:169-395).  cost: level-0 data from
+ * qm_cost_volume (read only).  sparse: device f32 width*height; the pixel
+ * (4x, 4y) of every quadtree-node cell receives its depth, all other pixels
+ * are left as they are (the reference writes into debug_image,
+ * seed_matrix.cu:530).  labels: device int32 (height/4)*(width/4) winning
+ * hypothesis per cell, -1 where the cell is not a node origin (NULL to
+ * skip).  messages: device f32 4*(height/4)*(width/4)*num_hyp final level-0
+ * messages in the order up, down, left, right (NULL to skip). */
+int qm_bp_workspace_size(int width, int height, const qm_params *p, size_t *bytes);
+int qm_bp_extract(const float *cost, int width, int height, const uint8_t *levels,
+                  const qm_params *p, float *sparse, int32_t *labels, float *messages,
+                  void *workspace, size_t workspace_bytes, void *stream);
+
+/* global_upsample (depth_upsample.cu:20-57) with build_weight_row/col,
+ * smooth_row and smooth_col (depth_upsample.cu:58-302).  dense: device f32
+ * width*height.  Needs width % 16 == 0 and height % 8 == 0 (the reference
+ * leaves the tails unwritten, depth_upsample.cu:111,216). */
+int qm_upsample_workspace_size(int width, int height, size_t *bytes);
+int qm_upsample(const float *sparse, const uint8_t *img, size_t img_pitch, int width, int height,
+                const qm_params *p, float *dense, void *workspace, size_t workspace_bytes,
+                void *stream);
+
+/* fuse_transform, hole_filling and fuse_currentmap (depth_fusion.cu:48-213;
+ * launch seed_matrix.cu:553-597).  depth: device f32 width*height, in:
+ * upsampled depth, out: fused depth (mu' or -1).  seeds_in / seeds_out:
+ * device float4 (a, b, mu, sigma^2) per pixel (seeds_in is rewritten with
+ * the transformed seeds, as the reference does).  T_income_last: HOST 12
+ * floats.  table: device int32 width*height (out: source pixel index per
+ * pixel, 0 = none). */
+int qm_fuse_workspace_size(int width, int height, size_t *bytes);
+int qm_fuse(float *depth, float *seeds_in, float *seeds_out, const float T_income_last[12],
+            const qm_camera *cam, int width, int height, const qm_params *p, int32_t *table,
+            void *workspace, size_t workspace_bytes, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QM_CAPI_H */

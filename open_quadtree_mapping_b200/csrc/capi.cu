@@ -1,0 +1,578 @@
+// extern "C" entry points of libqm_b200.so (declared in include/qm_capi.h).
+// Every entry point catches all exceptions and returns a status code; the
+// message is kept per thread for qm_last_error().
+#include <cstring>
+#include <new>
+
+#include "streams.h"
+
+namespace qm
+{
+namespace stage
+{
+Batch single(const JobDesc &J);
+int run_range(const Batch &B, const Shape &s, const qm_params &p, int first, int last,
+              cudaStream_t stream);
+int first_of(const char *name, int L);
+int last_of(const char *name, int L);
+} // namespace stage
+} // namespace qm
+
+struct qm_depthmap
+{
+  std::unique_ptr<qm::StreamSet> set;
+  float fx, fy, cx, cy;
+  int width, height;
+};
+
+struct qm_batch
+{
+  std::unique_ptr<qm::StreamSet> set;
+};
+
+namespace
+{
+
+using qm::CudaError;
+
+template <class F>
+int guarded(F &&f)
+{
+  try
+  {
+    f();
+    qm::set_error("");
+    return QM_OK;
+  }
+  catch (const CudaError &e)
+  {
+    qm::set_error(e.msg);
+    return e.status;
+  }
+  catch (const std::bad_alloc &)
+  {
+    qm::set_error("host allocation failed");
+    return QM_ERR_NO_MEMORY;
+  }
+  catch (const std::exception &e)
+  {
+    qm::set_error(e.what());
+    return QM_ERR_CUDA;
+  }
+  catch (...)
+  {
+    qm::set_error("unknown error");
+    return QM_ERR_CUDA;
+  }
+}
+
+void require(bool ok, const char *msg)
+{
+  if (!ok)
+    throw CudaError{QM_ERR_INVALID_ARG, msg};
+}
+
+qm_params params_or_default(const qm_params *p)
+{
+  qm_params q;
+  if (p)
+    q = *p;
+  else
+    qm_params_default(&q);
+  const std::string err = qm::validate(q);
+  require(err.empty(), err.c_str());
+  return q;
+}
+
+cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+size_t bp_workspace(int W, int H, const qm_params &p)
+{
+  size_t o = 0;
+  int w = W / 4, h = H / 4;
+  for (int l = 0; l < p.bp_levels; ++l)
+  {
+    const size_t n = (size_t)w * h * p.num_hyp * sizeof(float);
+    if (l > 0)
+      o += align256(n);
+    o += 4 * align256(n);
+    w = (w + 1) / 2;
+    h = (h + 1) / 2;
+  }
+  return o;
+}
+
+size_t upsample_workspace(int W, int H)
+{
+  const size_t P = (size_t)W * H;
+  return align256((size_t)(W + 1) * H * 4) + align256((size_t)W * (H + 1) * 4) +
+         align256(P * 3 * 8) + align256(P * 8);
+}
+
+size_t fuse_workspace(int W, int H) { return align256((size_t)W * H * 8); }
+
+void check_stage_size(int W, int H)
+{
+  require(W >= 8 && H >= 8 && W <= 16384 && H <= 16384, "image size must be within [8, 16384]");
+}
+
+qm::JobDesc base_desc(int W, int H, const qm_params &p)
+{
+  qm::JobDesc J;
+  std::memset(&J, 0, sizeof(J));
+  J.W = W;
+  J.H = H;
+  J.D = p.num_hyp;
+  J.F = 1;
+  J.cw = W / 4;
+  J.ch = H / 4;
+  J.min_inv = p.min_inv_depth;
+  J.step = p.inv_depth_step;
+  J.nlev = p.bp_levels;
+  return J;
+}
+
+qm::Shape stage_shape(int W, int H, const qm_params &p, int F, const qm_camera *cam)
+{
+  qm::Shape s;
+  s.W = W;
+  s.H = H;
+  s.D = p.num_hyp;
+  s.F = F;
+  s.cam = cam ? qm::Cam{cam->fx, cam->fy, cam->cx, cam->cy} : qm::Cam{1, 1, 0, 0};
+  return s;
+}
+
+void run_stage(const qm::JobDesc &J, const qm_params &p, const qm::Shape &s, const char *name,
+               void *stream, const qm::SlotInline *slots = nullptr)
+{
+  qm::Batch B = qm::stage::single(J);
+  if (slots)
+    B.slots = *slots;
+  qm::stage::run_range(B, s, p, qm::stage::first_of(name, p.bp_levels),
+                       qm::stage::last_of(name, p.bp_levels), as_stream(stream));
+}
+
+} // namespace
+
+extern "C" {
+
+void qm_params_default(qm_params *p)
+{
+  if (!p)
+    return;
+  std::memset(p, 0, sizeof(*p));
+  p->num_hyp = 64;
+  p->min_inv_depth = 0.01;
+  p->inv_depth_step = (2.0 - 0.01) / 63.0;
+  p->P1 = 0.003f;
+  p->P2 = 0.01f;
+  p->bp_levels = 4;
+  p->bp_iters[0] = 4;
+  p->bp_iters[1] = 10;
+  p->bp_iters[2] = 10;
+  p->bp_iters[3] = 10;
+  p->qt_max_level = 4;
+  p->qt_min_level = 2;
+  p->qt_threshold = 10.0f;
+  p->up_sigma = 400.0;
+  p->up_lambda = 10.0;
+  p->arith = QM_ARITH_REFERENCE;
+}
+
+const char *qm_last_error(void) { return qm::get_error(); }
+
+int qm_version(void) { return 100; }
+
+// ------------------------------------------------------------ facade
+
+int qm_depthmap_create(qm_depthmap **out, int width, int height, float fx, float cx, float fy,
+                       float cy, int semi2dense_ratio, const qm_params *params, int device)
+{
+  return guarded([&] {
+    require(out != nullptr, "out is NULL");
+    *out = nullptr;
+    const qm_params p = params_or_default(params);
+    qm::StreamDesc d;
+    d.W = width;
+    d.H = height;
+    d.cam = qm::Cam{fx, fy, cx, cy};
+    d.D = p.num_hyp;
+    d.F = 5; // measurement slots of the reference launch (seed_matrix.cu:505)
+    d.ratio = semi2dense_ratio;
+    auto h = std::make_unique<qm_depthmap>();
+    h->set = std::make_unique<qm::StreamSet>(device, p, std::vector<qm::StreamDesc>{d});
+    h->fx = fx;
+    h->fy = fy;
+    h->cx = cx;
+    h->cy = cy;
+    h->width = width;
+    h->height = height;
+    *out = h.release();
+  });
+}
+
+int qm_depthmap_destroy(qm_depthmap *h)
+{
+  return guarded([&] { delete h; });
+}
+
+int qm_depthmap_add_frame(qm_depthmap *h, const uint8_t *img, size_t stride,
+                          const float T_curr_world[12], int *has_result)
+{
+  return guarded([&] {
+    require(h && img && T_curr_world && has_result, "NULL argument");
+    std::lock_guard<std::mutex> lock(h->set->mutex());
+    *has_result = h->set->add_frame(0, img, stride, T_curr_world);
+  });
+}
+
+int qm_depthmap_get_depth(qm_depthmap *h, float *out, size_t stride)
+{
+  return guarded([&] {
+    require(h && out && stride >= (size_t)h->width, "bad argument");
+    std::lock_guard<std::mutex> lock(h->set->mutex());
+    h->set->get_depth(0, out, stride);
+  });
+}
+
+int qm_depthmap_get_debug(qm_depthmap *h, float *out, size_t stride)
+{
+  return guarded([&] {
+    require(h && out && stride >= (size_t)h->width, "bad argument");
+    std::lock_guard<std::mutex> lock(h->set->mutex());
+    h->set->get_debug(0, out, stride);
+  });
+}
+
+int qm_depthmap_get_reference(qm_depthmap *h, uint8_t *out, size_t stride)
+{
+  return guarded([&] {
+    require(h && out && stride >= (size_t)h->width, "bad argument");
+    std::lock_guard<std::mutex> lock(h->set->mutex());
+    h->set->get_reference(0, out, stride);
+  });
+}
+
+int qm_depthmap_get_T_world_ref(qm_depthmap *h, float T[12])
+{
+  return guarded([&] {
+    require(h && T, "NULL argument");
+    std::lock_guard<std::mutex> lock(h->set->mutex());
+    h->set->get_T_world_ref(0, T);
+  });
+}
+
+int qm_depthmap_get_camera(qm_depthmap *h, qm_camera *cam, int *width, int *height)
+{
+  return guarded([&] {
+    require(h != nullptr, "NULL handle");
+    if (cam)
+      *cam = qm_camera{h->fx, h->fy, h->cx, h->cy};
+    if (width)
+      *width = h->width;
+    if (height)
+      *height = h->height;
+  });
+}
+
+// ------------------------------------------------------------- batch
+
+int qm_batch_create(qm_batch **out, int num_streams, const qm_stream_desc *descs,
+                    const qm_params *params, int device)
+{
+  return guarded([&] {
+    require(out != nullptr, "out is NULL");
+    *out = nullptr;
+    require(num_streams >= 1 && descs != nullptr, "need at least one stream");
+    const qm_params p = params_or_default(params);
+    std::vector<qm::StreamDesc> ds;
+    for (int i = 0; i < num_streams; ++i)
+    {
+      const qm_stream_desc &s = descs[i];
+      qm::StreamDesc d;
+      d.W = s.width;
+      d.H = s.height;
+      d.cam = qm::Cam{s.cam.fx, s.cam.fy, s.cam.cx, s.cam.cy};
+      d.D = s.num_hyp > 0 ? s.num_hyp : p.num_hyp;
+      d.F = s.num_slots > 0 ? s.num_slots : 5;
+      d.ratio = s.semi2dense_ratio > 0 ? s.semi2dense_ratio : 1;
+      ds.push_back(d);
+    }
+    auto b = std::make_unique<qm_batch>();
+    b->set = std::make_unique<qm::StreamSet>(device, p, ds);
+    *out = b.release();
+  });
+}
+
+int qm_batch_destroy(qm_batch *b)
+{
+  return guarded([&] { delete b; });
+}
+
+int qm_batch_add_frames(qm_batch *b, const uint8_t *const *imgs, const size_t *strides,
+                        const float *T_curr_world, int *has_result)
+{
+  return guarded([&] {
+    require(b && imgs && strides && T_curr_world && has_result, "NULL argument");
+    std::lock_guard<std::mutex> lock(b->set->mutex());
+    b->set->add_frames(imgs, strides, T_curr_world, has_result);
+  });
+}
+
+int qm_batch_get_depth(qm_batch *b, int stream, float *out, size_t stride)
+{
+  return guarded([&] {
+    require(b && out && stream >= 0 && stream < b->set->size(), "bad argument");
+    require(stride >= (size_t)b->set->desc(stream).W, "stride too small");
+    std::lock_guard<std::mutex> lock(b->set->mutex());
+    b->set->get_depth(stream, out, stride);
+  });
+}
+
+int qm_batch_get_debug(qm_batch *b, int stream, float *out, size_t stride)
+{
+  return guarded([&] {
+    require(b && out && stream >= 0 && stream < b->set->size(), "bad argument");
+    require(stride >= (size_t)b->set->desc(stream).W, "stride too small");
+    std::lock_guard<std::mutex> lock(b->set->mutex());
+    b->set->get_debug(stream, out, stride);
+  });
+}
+
+int qm_batch_run_resident(qm_batch *b)
+{
+  return guarded([&] {
+    require(b != nullptr, "NULL handle");
+    std::lock_guard<std::mutex> lock(b->set->mutex());
+    b->set->run_resident();
+  });
+}
+
+int qm_batch_device_depth(qm_batch *b, int stream, const float **dev_ptr)
+{
+  return guarded([&] {
+    require(b && dev_ptr && stream >= 0 && stream < b->set->size(), "bad argument");
+    *dev_ptr = b->set->device_depth(stream);
+  });
+}
+
+int qm_batch_set_graphs(qm_batch *b, int enable)
+{
+  return guarded([&] {
+    require(b != nullptr, "NULL handle");
+    b->set->engine().set_graphs(enable != 0);
+  });
+}
+
+int qm_batch_last_launches(qm_batch *b, int *count)
+{
+  return guarded([&] {
+    require(b && count, "NULL argument");
+    *count = b->set->engine().last_launches();
+  });
+}
+
+int qm_batch_stream(qm_batch *b, void **stream)
+{
+  return guarded([&] {
+    require(b && stream, "NULL argument");
+    *stream = reinterpret_cast<void *>(b->set->engine().stream());
+  });
+}
+
+int qm_batch_profile(qm_batch *b, float ms[QM_NUM_KERNEL_KINDS],
+                     int launches[QM_NUM_KERNEL_KINDS])
+{
+  static_assert(QM_NUM_KERNEL_KINDS == qm::kNumKinds, "kernel kind count");
+  return guarded([&] {
+    require(b && ms && launches, "NULL argument");
+    std::lock_guard<std::mutex> lock(b->set->mutex());
+    b->set->profile_resident(ms, launches);
+  });
+}
+
+// ------------------------------------------------------------ stages
+
+int qm_quadtree(const uint8_t *img, size_t img_pitch, int width, int height, const qm_params *p,
+                uint8_t *levels, void *stream)
+{
+  return guarded([&] {
+    check_stage_size(width, height);
+    require(img && levels && img_pitch >= (size_t)width, "bad argument");
+    const qm_params q = params_or_default(p);
+    qm::JobDesc J = base_desc(width, height, q);
+    J.ref = img;
+    J.ref_pitch = (int)img_pitch;
+    J.levels = levels;
+    run_stage(J, q, stage_shape(width, height, q, 1, nullptr), "quadtree", stream);
+  });
+}
+
+int qm_cost_volume(const uint8_t *ref, size_t ref_pitch, int width, int height,
+                   const qm_camera *cam, const uint8_t *levels, int num_slots,
+                   const uint8_t *const *slots, size_t slot_pitch, const float *T_slot_ref,
+                   const qm_params *p, float *cost, void *stream)
+{
+  return guarded([&] {
+    check_stage_size(width, height);
+    require(ref && cam && levels && slots && T_slot_ref && cost, "NULL argument");
+    require(ref_pitch >= (size_t)width && slot_pitch >= (size_t)width, "pitch too small");
+    require(num_slots >= 1 && num_slots <= QM_MAX_SLOTS, "num_slots must be in [1, 32]");
+    const qm_params q = params_or_default(p);
+    qm::JobDesc J = base_desc(width, height, q);
+    J.F = num_slots;
+    J.fx = cam->fx;
+    J.fy = cam->fy;
+    J.cx = cam->cx;
+    J.cy = cam->cy;
+    J.ref = ref;
+    J.ref_pitch = (int)ref_pitch;
+    J.slot_pitch = (int)slot_pitch;
+    J.levels = const_cast<uint8_t *>(levels);
+    J.lv[0].data = cost;
+    qm::SlotInline si;
+    std::memset(&si, 0, sizeof(si));
+    for (int f = 0; f < num_slots; ++f)
+    {
+      require(slots[f] != nullptr, "NULL slot image");
+      si.ptr[f] = slots[f];
+      std::memcpy(si.T + 12 * f, T_slot_ref + 12 * f, 12 * sizeof(float));
+    }
+    run_stage(J, q, stage_shape(width, height, q, num_slots, cam), "cost", stream, &si);
+  });
+}
+
+int qm_bp_workspace_size(int width, int height, const qm_params *p, size_t *bytes)
+{
+  return guarded([&] {
+    check_stage_size(width, height);
+    require(bytes != nullptr, "NULL argument");
+    const qm_params q = params_or_default(p);
+    *bytes = bp_workspace(width, height, q);
+  });
+}
+
+int qm_bp_extract(const float *cost, int width, int height, const uint8_t *levels,
+                  const qm_params *p, float *sparse, int32_t *labels, float *messages,
+                  void *workspace, size_t workspace_bytes, void *stream)
+{
+  return guarded([&] {
+    check_stage_size(width, height);
+    require(cost && levels && sparse, "NULL argument");
+    const qm_params q = params_or_default(p);
+    const size_t need = bp_workspace(width, height, q);
+    if (workspace_bytes < need || !workspace)
+      throw CudaError{QM_ERR_WORKSPACE, "BP workspace too small"};
+    qm::JobDesc J = base_desc(width, height, q);
+    J.levels = const_cast<uint8_t *>(levels);
+    J.sparse = sparse;
+    J.labels = labels;
+    char *ws = (char *)workspace;
+    size_t o = 0;
+    int w = width / 4, h = height / 4;
+    for (int l = 0; l < q.bp_levels; ++l)
+    {
+      const size_t n = (size_t)w * h * q.num_hyp * sizeof(float);
+      J.lv[l].w = w;
+      J.lv[l].h = h;
+      if (l == 0)
+        J.lv[l].data = const_cast<float *>(cost);
+      else
+      {
+        J.lv[l].data = (float *)(ws + o);
+        o += align256(n);
+      }
+      for (int m = 0; m < 4; ++m)
+      {
+        J.lv[l].msg[m] = (float *)(ws + o);
+        o += align256(n);
+        if (l == 0 && messages)
+          J.lv[l].msg[m] = messages + (size_t)m * w * h * q.num_hyp;
+      }
+      w = (w + 1) / 2;
+      h = (h + 1) / 2;
+    }
+    run_stage(J, q, stage_shape(width, height, q, 1, nullptr), "bp", stream);
+  });
+}
+
+int qm_upsample_workspace_size(int width, int height, size_t *bytes)
+{
+  return guarded([&] {
+    check_stage_size(width, height);
+    require(bytes != nullptr, "NULL argument");
+    *bytes = upsample_workspace(width, height);
+  });
+}
+
+int qm_upsample(const float *sparse, const uint8_t *img, size_t img_pitch, int width, int height,
+                const qm_params *p, float *dense, void *workspace, size_t workspace_bytes,
+                void *stream)
+{
+  return guarded([&] {
+    check_stage_size(width, height);
+    require(width % 16 == 0 && height % 8 == 0,
+            "width must be a multiple of 16 and height of 8");
+    require(sparse && img && dense && img_pitch >= (size_t)width, "bad argument");
+    const qm_params q = params_or_default(p);
+    const size_t P = (size_t)width * height;
+    if (workspace_bytes < upsample_workspace(width, height) || !workspace)
+      throw CudaError{QM_ERR_WORKSPACE, "upsample workspace too small"};
+    qm::JobDesc J = base_desc(width, height, q);
+    J.ref = img;
+    J.ref_pitch = (int)img_pitch;
+    J.sparse = const_cast<float *>(sparse);
+    J.dense = dense;
+    char *ws = (char *)workspace;
+    size_t o = 0;
+    J.row_w = (float *)(ws + o);
+    o += align256((size_t)(width + 1) * height * 4);
+    J.col_w = (float *)(ws + o);
+    o += align256((size_t)width * (height + 1) * 4);
+    J.tmp = (double *)(ws + o);
+    o += align256(P * 3 * 8);
+    J.rowres = (float2 *)(ws + o);
+    run_stage(J, q, stage_shape(width, height, q, 1, nullptr), "upsample", stream);
+  });
+}
+
+int qm_fuse_workspace_size(int width, int height, size_t *bytes)
+{
+  return guarded([&] {
+    check_stage_size(width, height);
+    require(bytes != nullptr, "NULL argument");
+    *bytes = fuse_workspace(width, height);
+  });
+}
+
+int qm_fuse(float *depth, float *seeds_in, float *seeds_out, const float T_income_last[12],
+            const qm_camera *cam, int width, int height, const qm_params *p, int32_t *table,
+            void *workspace, size_t workspace_bytes, void *stream)
+{
+  return guarded([&] {
+    check_stage_size(width, height);
+    require(depth && seeds_in && seeds_out && T_income_last && cam && table, "NULL argument");
+    const qm_params q = params_or_default(p);
+    if (workspace_bytes < fuse_workspace(width, height) || !workspace)
+      throw CudaError{QM_ERR_WORKSPACE, "fuse workspace too small"};
+    qm::JobDesc J = base_desc(width, height, q);
+    J.fx = cam->fx;
+    J.fy = cam->fy;
+    J.cx = cam->cx;
+    J.cy = cam->cy;
+    J.dense = depth;
+    J.seeds_in = reinterpret_cast<float4 *>(seeds_in);
+    J.seeds_out = reinterpret_cast<float4 *>(seeds_out);
+    J.table = table;
+    J.zkey = (unsigned long long *)workspace;
+    std::memcpy(J.Tf, T_income_last, 12 * sizeof(float));
+    qm::check(cudaMemsetAsync(workspace, 0xff, fuse_workspace(width, height), as_stream(stream)),
+              "workspace reset");
+    run_stage(J, q, stage_shape(width, height, q, 1, cam), "fuse", stream);
+  });
+}
+
+} // extern "C"

@@ -1,0 +1,697 @@
+// Host engine of the dense pipeline (see engine.h).
+//
+// Stage order of one run, after SeedMatrix::extract_depth and
+// fuse_output_depth (seed_matrix.cu:448-597):
+//   quadtree -> cost -> pyramid(1..L-1) -> zero messages(L-1) ->
+//   for level L-1..0: [message upsample] + bp half-sweeps ->
+//   extraction -> weights -> row solve -> column solve ->
+//   fuse transform -> hole fill -> fuse update.
+// Every stage is one launch over all active jobs (one per hypothesis count
+// for the warp-per-cell BP kernels).  The reference runs 60-70 launches per
+// keyframe with a cudaDeviceSynchronize after most and ~25 device
+// allocations; here a keyframe batch is ~45 launches, no allocation, and the
+// whole sequence is captured once per active set and replayed as a graph.
+#include "engine.h"
+
+#include <algorithm>
+#include <cstring>
+#include <set>
+
+namespace qm
+{
+
+namespace
+{
+thread_local std::string t_err;
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+int cdiv(long a, long b) { return (int)((a + b - 1) / b); }
+
+// Stage indices for L pyramid levels.
+struct Stages
+{
+  int L;
+  int qt() const { return 0; }
+  int cost() const { return 1; }
+  int pyr(int l) const { return 2 + (l - 1); } // l = 1..L-1
+  int mzero() const { return 1 + L; }
+  int mup(int l) const { return 2 + L + l; } // l = 0..L-2
+  int sweep(int l) const { return 1 + 2 * L + l; }
+  int extract() const { return 1 + 3 * L; }
+  int weights() const { return 2 + 3 * L; }
+  int row() const { return 3 + 3 * L; }
+  int col() const { return 4 + 3 * L; }
+  int ftrans() const { return 5 + 3 * L; }
+  int ffill() const { return 6 + 3 * L; }
+  int fupd() const { return 7 + 3 * L; }
+  int count() const { return 8 + 3 * L; }
+};
+
+std::vector<int> stage_blocks(const Shape &s, const JobLayout &lay, const qm_params &p)
+{
+  const Stages st{p.bp_levels};
+  std::vector<int> b(st.count(), 0);
+  const int L = p.bp_levels;
+  const int T = quadtree_tile(p.qt_max_level);
+  const int D = s.D;
+  b[st.qt()] = cdiv(s.W, T) * cdiv(s.H, T);
+  b[st.cost()] = cdiv((long)lay.lw[0] * lay.lh[0] * D, kFlatThreads);
+  for (int l = 1; l < L; ++l)
+    b[st.pyr(l)] = cdiv((long)lay.lw[l] * lay.lh[l] * D, kFlatThreads);
+  b[st.mzero()] = cdiv((long)lay.lw[L - 1] * lay.lh[L - 1] * D, kFlatThreads);
+  for (int l = 0; l + 1 < L; ++l)
+    b[st.mup(l)] = cdiv((long)lay.lw[l] * lay.lh[l] * D, kFlatThreads);
+  for (int l = 0; l < L; ++l)
+    b[st.sweep(l)] = cdiv((long)((lay.lw[l] + 1) / 2) * lay.lh[l], kCellWarps);
+  b[st.extract()] = cdiv((long)lay.lw[0] * lay.lh[0], kCellWarps);
+  b[st.weights()] = cdiv((long)(s.W + 1) * (s.H + 1), kFlatThreads);
+  b[st.row()] = cdiv(s.H, kLineThreads);
+  b[st.col()] = cdiv(s.W, kLineThreads);
+  b[st.ftrans()] = b[st.ffill()] = b[st.fupd()] = cdiv((long)s.W * s.H, kFlatThreads);
+  return b;
+}
+
+// Launches stages [first, last] of the sequence; B.prefix is replaced by
+// prefix[stage] (may be null for a single inline job).  When `prof` is given,
+// every launch is bracketed by a pair of events recorded on `s`.  Returns the
+// number of kernel launches.
+int enqueue_range(Batch B, const std::vector<const int *> &prefix, const std::vector<int> &blocks,
+                  const qm_params &p, const std::vector<int> &dvals, int first, int last,
+                  cudaStream_t s, LaunchProfile *prof = nullptr)
+{
+  const Stages st{p.bp_levels};
+  const int L = p.bp_levels;
+  const KParams kp = kparams(p);
+  const int ar = p.arith;
+  int n = 0;
+  auto in = [&](int stage) { return stage >= first && stage <= last && blocks[stage] > 0; };
+  auto at = [&](int stage) {
+    Batch b = B;
+    b.prefix = prefix.empty() ? nullptr : prefix[stage];
+    return b;
+  };
+  auto launch = [&](int kind, auto &&fn) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (prof)
+    {
+      check(cudaEventCreate(&e0), "event");
+      check(cudaEventCreate(&e1), "event");
+      check(cudaEventRecord(e0, s), "event");
+    }
+    fn();
+    if (prof)
+    {
+      check(cudaEventRecord(e1, s), "event");
+      prof->marks.push_back({kind, e0, e1});
+    }
+    ++n;
+  };
+  if (in(st.qt()))
+    launch(kQuadtree, [&] { launch_quadtree(at(st.qt()), blocks[st.qt()], kp, s); });
+  if (in(st.cost()))
+    launch(kCost, [&] { launch_cost(at(st.cost()), blocks[st.cost()], ar, s); });
+  for (int l = 1; l < L; ++l)
+    if (in(st.pyr(l)))
+      launch(kPyramid, [&] { launch_pyramid(at(st.pyr(l)), blocks[st.pyr(l)], l, s); });
+  if (in(st.mzero()))
+    launch(kMsgInit, [&] { launch_msg_zero(at(st.mzero()), blocks[st.mzero()], L - 1, s); });
+  for (int l = L - 1; l >= 0; --l)
+  {
+    if (l + 1 < L && in(st.mup(l)))
+      launch(kMsgInit, [&] { launch_msg_upsample(at(st.mup(l)), blocks[st.mup(l)], l, s); });
+    if (in(st.sweep(l)))
+      for (int it = 0; it < p.bp_iters[l]; ++it)
+        for (int d : dvals)
+          launch(kSweep, [&] {
+            launch_bp_sweep(at(st.sweep(l)), blocks[st.sweep(l)], d, l, it & 1, kp, ar, s);
+          });
+  }
+  if (in(st.extract()))
+    for (int d : dvals)
+      launch(kExtract, [&] { launch_extract(at(st.extract()), blocks[st.extract()], d, ar, s); });
+  if (in(st.weights()))
+    launch(kWeights, [&] { launch_weights(at(st.weights()), blocks[st.weights()], kp, ar, s); });
+  if (in(st.row()))
+    launch(kRowSolve, [&] { launch_row_solve(at(st.row()), blocks[st.row()], kp, s); });
+  if (in(st.col()))
+    launch(kColSolve, [&] { launch_col_solve(at(st.col()), blocks[st.col()], kp, s); });
+  if (in(st.ftrans()))
+    launch(kFuseTransform,
+           [&] { launch_fuse_transform(at(st.ftrans()), blocks[st.ftrans()], ar, s); });
+  if (in(st.ffill()))
+    launch(kFuseFill, [&] { launch_fuse_fill(at(st.ffill()), blocks[st.ffill()], s); });
+  if (in(st.fupd()))
+    launch(kFuseUpdate, [&] { launch_fuse_update(at(st.fupd()), blocks[st.fupd()], s); });
+  check(cudaGetLastError(), "kernel launch");
+  return n;
+}
+
+} // namespace
+
+void set_error(const std::string &msg) { t_err = msg; }
+const char *get_error() { return t_err.c_str(); }
+
+void check(cudaError_t e, const char *what)
+{
+  if (e != cudaSuccess)
+  {
+    cudaGetLastError(); // clear a sticky launch error of this call
+    throw CudaError{e == cudaErrorMemoryAllocation ? QM_ERR_NO_MEMORY : QM_ERR_CUDA,
+                    std::string(what) + ": " + cudaGetErrorString(e)};
+  }
+}
+
+KParams kparams(const qm_params &p)
+{
+  KParams k;
+  k.P1 = p.P1;
+  k.P2 = p.P2;
+  k.qt_max = p.qt_max_level;
+  k.qt_min = p.qt_min_level;
+  k.qt_thr = p.qt_threshold;
+  k.up_sigma = p.up_sigma;
+  k.up_lambda = p.up_lambda;
+  return k;
+}
+
+std::string validate(const qm_params &p)
+{
+  if (!bp_supported_d(p.num_hyp))
+    return "num_hyp must be one of 32, 48, 64, 96, 128";
+  if (p.bp_levels < 1 || p.bp_levels > kMaxLevels)
+    return "bp_levels must be in [1, 8]";
+  for (int l = 0; l < p.bp_levels; ++l)
+    if (p.bp_iters[l] < 0 || p.bp_iters[l] > 1000)
+      return "bp_iters out of range";
+  if (p.qt_max_level < 1 || p.qt_max_level > 5)
+    return "qt_max_level must be in [1, 5]";
+  if (p.qt_min_level < 0 || p.qt_min_level > p.qt_max_level)
+    return "qt_min_level must be in [0, qt_max_level]";
+  if (!(p.inv_depth_step > 0.0) || !(p.min_inv_depth > 0.0))
+    return "inverse-depth range must be positive";
+  if (!(p.up_sigma > 0.0) || !(p.up_lambda >= 0.0))
+    return "upsample sigma/lambda out of range";
+  if (p.arith != QM_ARITH_REFERENCE && p.arith != QM_ARITH_IEEE)
+    return "arith must be QM_ARITH_REFERENCE or QM_ARITH_IEEE";
+  return "";
+}
+
+std::string validate(const Shape &s, const qm_params &p)
+{
+  if (s.W < 16 || s.H < 16 || s.W > 16384 || s.H > 16384)
+    return "image size must be within [16, 16384]";
+  if (s.W % 16 != 0 || s.H % 8 != 0)
+    return "width must be a multiple of 16 and height of 8 (the upsampler's line chunks)";
+  if (!bp_supported_d(s.D))
+    return "num_hyp must be one of 32, 48, 64, 96, 128";
+  if (s.F < 1 || s.F > kMaxSlots)
+    return "num_slots must be in [1, 32]";
+  if (!(s.cam.fx > 0.0f) || !(s.cam.fy > 0.0f))
+    return "focal lengths must be positive";
+  (void)p;
+  return "";
+}
+
+JobLayout JobLayout::make(const Shape &s, int nlev)
+{
+  JobLayout L;
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    const size_t r = o;
+    o = align256(o + bytes);
+    return r;
+  };
+  const size_t P = (size_t)s.W * s.H;
+  L.off_levels = take(P);
+  int w = s.W / 4, h = s.H / 4;
+  for (int l = 0; l < kMaxLevels; ++l)
+  {
+    L.lw[l] = w;
+    L.lh[l] = h;
+    if (l < nlev)
+    {
+      const size_t n = (size_t)w * h * s.D * sizeof(float);
+      L.off_data[l] = take(n);
+      for (int m = 0; m < 4; ++m)
+        L.off_msg[l][m] = take(n);
+    }
+    w = (w + 1) / 2;
+    h = (h + 1) / 2;
+  }
+  L.off_labels = take((size_t)(s.W / 4) * (s.H / 4) * sizeof(int32_t));
+  L.off_sparse = take(P * sizeof(float));
+  L.off_dense = take(P * sizeof(float));
+  L.off_row_w = take((size_t)(s.W + 1) * s.H * sizeof(float));
+  L.off_col_w = take((size_t)s.W * (s.H + 1) * sizeof(float));
+  L.off_tmp = take(P * 3 * sizeof(double));
+  L.off_rowres = take(P * sizeof(float2));
+  L.off_seeds[0] = take(P * sizeof(float4));
+  L.off_seeds[1] = take(P * sizeof(float4));
+  L.off_zkey = take(P * sizeof(unsigned long long));
+  L.off_table = take(P * sizeof(int32_t));
+  L.bytes = o;
+  return L;
+}
+
+JobDesc make_job_desc(const Shape &s, const qm_params &p, const JobBuffers &b, int seeds_cur)
+{
+  JobDesc J;
+  std::memset(&J, 0, sizeof(J));
+  J.W = s.W;
+  J.H = s.H;
+  J.D = s.D;
+  J.F = s.F;
+  J.cw = s.W / 4;
+  J.ch = s.H / 4;
+  J.fx = s.cam.fx;
+  J.fy = s.cam.fy;
+  J.cx = s.cam.cx;
+  J.cy = s.cam.cy;
+  J.min_inv = p.min_inv_depth;
+  J.step = p.inv_depth_step;
+  J.levels = b.levels;
+  J.nlev = p.bp_levels;
+  for (int l = 0; l < p.bp_levels; ++l)
+  {
+    J.lv[l].w = b.lw[l];
+    J.lv[l].h = b.lh[l];
+    J.lv[l].data = b.data[l];
+    for (int m = 0; m < 4; ++m)
+      J.lv[l].msg[m] = b.msg[l][m];
+  }
+  J.labels = b.labels;
+  J.sparse = b.sparse;
+  J.dense = b.dense;
+  J.row_w = b.row_w;
+  J.col_w = b.col_w;
+  J.tmp = b.tmp;
+  J.rowres = b.rowres;
+  J.seeds_in = b.seeds[seeds_cur];
+  J.seeds_out = b.seeds[seeds_cur ^ 1];
+  J.zkey = b.zkey;
+  J.table = b.table;
+  for (int k = 0; k < 12; ++k)
+    J.Tf[k] = (k == 0 || k == 5 || k == 10) ? 1.0f : 0.0f;
+  return J;
+}
+
+struct Plan
+{
+  std::vector<int> active;
+  int *d_prefix = nullptr;
+  std::vector<const int *> prefix; // per stage, into d_prefix
+  std::vector<int> blocks;         // per stage, total
+  std::vector<int> dvals;
+  cudaGraphExec_t exec = nullptr;
+  ~Plan()
+  {
+    if (exec)
+      cudaGraphExecDestroy(exec);
+    if (d_prefix)
+      cudaFree(d_prefix);
+  }
+};
+
+Engine::Engine(int device, const qm_params &p, const std::vector<Shape> &shapes)
+    : device_(device), params_(p), shapes_(shapes)
+{
+  std::string err = validate(p);
+  if (!err.empty())
+    throw CudaError{QM_ERR_INVALID_ARG, err};
+  if (shapes.empty())
+    throw CudaError{QM_ERR_INVALID_ARG, "no jobs"};
+  for (const auto &s : shapes)
+  {
+    err = validate(s, p);
+    if (!err.empty())
+      throw CudaError{QM_ERR_INVALID_ARG, err};
+  }
+  check(cudaSetDevice(device), "cudaSetDevice");
+  check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  check(cudaEventCreate(&ev0_), "cudaEventCreate");
+  check(cudaEventCreate(&ev1_), "cudaEventCreate");
+  const int n = njobs();
+  size_t total = 0;
+  std::vector<size_t> base(n);
+  for (int j = 0; j < n; ++j)
+  {
+    layouts_.push_back(JobLayout::make(shapes[j], p.bp_levels));
+    base[j] = total;
+    total += layouts_[j].bytes;
+  }
+  check(cudaMalloc(&arena_, total), "device workspace allocation");
+  bufs_.resize(n);
+  seeds_cur_.assign(n, 0);
+  for (int j = 0; j < n; ++j)
+  {
+    char *b0 = (char *)arena_ + base[j];
+    const JobLayout &L = layouts_[j];
+    JobBuffers &B = bufs_[j];
+    B.levels = (uint8_t *)(b0 + L.off_levels);
+    for (int l = 0; l < p.bp_levels; ++l)
+    {
+      B.data[l] = (float *)(b0 + L.off_data[l]);
+      for (int m = 0; m < 4; ++m)
+        B.msg[l][m] = (float *)(b0 + L.off_msg[l][m]);
+    }
+    for (int l = 0; l < kMaxLevels; ++l)
+    {
+      B.lw[l] = L.lw[l];
+      B.lh[l] = L.lh[l];
+    }
+    B.labels = (int32_t *)(b0 + L.off_labels);
+    B.sparse = (float *)(b0 + L.off_sparse);
+    B.dense = (float *)(b0 + L.off_dense);
+    B.row_w = (float *)(b0 + L.off_row_w);
+    B.col_w = (float *)(b0 + L.off_col_w);
+    B.tmp = (double *)(b0 + L.off_tmp);
+    B.rowres = (float2 *)(b0 + L.off_rowres);
+    B.seeds[0] = (float4 *)(b0 + L.off_seeds[0]);
+    B.seeds[1] = (float4 *)(b0 + L.off_seeds[1]);
+    B.zkey = (unsigned long long *)(b0 + L.off_zkey);
+    B.table = (int32_t *)(b0 + L.off_table);
+    const size_t P = (size_t)shapes[j].W * shapes[j].H;
+    check(cudaMemsetAsync(B.seeds[0], 0, P * sizeof(float4) * 1, stream_), "memset");
+    check(cudaMemsetAsync(B.seeds[1], 0, P * sizeof(float4) * 1, stream_), "memset");
+    check(cudaMemsetAsync(B.zkey, 0xff, P * sizeof(unsigned long long), stream_), "memset");
+    check(cudaMemsetAsync(B.sparse, 0, P * sizeof(float), stream_), "memset");
+    check(cudaMemsetAsync(B.dense, 0, P * sizeof(float), stream_), "memset");
+    check(cudaMemsetAsync(B.table, 0, P * sizeof(int32_t), stream_), "memset");
+  }
+  slot_base_.resize(n);
+  for (int j = 0; j < n; ++j)
+  {
+    slot_base_[j] = total_slots_;
+    total_slots_ += shapes[j].F;
+  }
+  check(cudaHostAlloc((void **)&h_slot_ptr_, sizeof(void *) * total_slots_, cudaHostAllocDefault),
+        "pinned allocation");
+  check(cudaHostAlloc((void **)&h_slot_T_, sizeof(float) * 12 * total_slots_, cudaHostAllocDefault),
+        "pinned allocation");
+  std::memset(h_slot_ptr_, 0, sizeof(void *) * total_slots_);
+  std::memset(h_slot_T_, 0, sizeof(float) * 12 * total_slots_);
+  check(cudaMalloc((void **)&d_slot_ptr_, sizeof(void *) * total_slots_), "device allocation");
+  check(cudaMalloc((void **)&d_slot_T_, sizeof(float) * 12 * total_slots_), "device allocation");
+  master_.resize(n);
+  for (int j = 0; j < n; ++j)
+  {
+    master_[j] = make_job_desc(shapes[j], p, bufs_[j], 0);
+    master_[j].slot_base = slot_base_[j];
+  }
+  check(cudaHostAlloc((void **)&h_run_, sizeof(JobDesc) * n, cudaHostAllocDefault),
+        "pinned allocation");
+  check(cudaMalloc((void **)&d_run_, sizeof(JobDesc) * n), "device allocation");
+  check(cudaStreamSynchronize(stream_), "engine init");
+}
+
+Engine::~Engine()
+{
+  cudaSetDevice(device_);
+  if (stream_)
+    cudaStreamSynchronize(stream_);
+  plans_.clear();
+  if (arena_)
+    cudaFree(arena_);
+  if (d_slot_ptr_)
+    cudaFree(d_slot_ptr_);
+  if (d_slot_T_)
+    cudaFree(d_slot_T_);
+  if (d_run_)
+    cudaFree(d_run_);
+  if (h_slot_ptr_)
+    cudaFreeHost(h_slot_ptr_);
+  if (h_slot_T_)
+    cudaFreeHost(h_slot_T_);
+  if (h_run_)
+    cudaFreeHost(h_run_);
+  if (ev0_)
+    cudaEventDestroy(ev0_);
+  if (ev1_)
+    cudaEventDestroy(ev1_);
+  if (stream_)
+    cudaStreamDestroy(stream_);
+}
+
+void Engine::set_inputs(int j, const uint8_t *ref, int ref_pitch, const uint8_t *const *slots,
+                        int slot_pitch, const float *T_slot_ref, const float *T_fuse)
+{
+  JobDesc &J = master_[j];
+  J.ref = ref;
+  J.ref_pitch = ref_pitch;
+  J.slot_pitch = slot_pitch;
+  for (int f = 0; f < shapes_[j].F; ++f)
+  {
+    h_slot_ptr_[slot_base_[j] + f] = slots[f];
+    std::memcpy(h_slot_T_ + 12 * (slot_base_[j] + f), T_slot_ref + 12 * f, 12 * sizeof(float));
+  }
+  if (T_fuse)
+    std::memcpy(J.Tf, T_fuse, 12 * sizeof(float));
+}
+
+void Engine::reset_seeds(int j)
+{
+  const size_t P = (size_t)shapes_[j].W * shapes_[j].H;
+  check(cudaMemsetAsync(bufs_[j].seeds[0], 0, P * sizeof(float4), stream_), "memset");
+  check(cudaMemsetAsync(bufs_[j].seeds[1], 0, P * sizeof(float4), stream_), "memset");
+  check(cudaStreamSynchronize(stream_), "reset seeds");
+  seeds_cur_[j] = 0;
+}
+
+Plan &Engine::plan_for(const std::vector<int> &active)
+{
+  auto it = plans_.find(active);
+  if (it != plans_.end())
+    return *it->second;
+  auto pl = std::make_unique<Plan>();
+  pl->active = active;
+  const Stages st{params_.bp_levels};
+  const int ns = st.count();
+  const int n = (int)active.size();
+  std::vector<int> h(ns * (n + 1), 0);
+  pl->blocks.assign(ns, 0);
+  std::set<int> ds;
+  for (int i = 0; i < n; ++i)
+  {
+    const int j = active[i];
+    ds.insert(shapes_[j].D);
+    const std::vector<int> b = stage_blocks(shapes_[j], layouts_[j], params_);
+    for (int s = 0; s < ns; ++s)
+      h[s * (n + 1) + i + 1] = h[s * (n + 1) + i] + b[s];
+  }
+  for (int s = 0; s < ns; ++s)
+    pl->blocks[s] = h[s * (n + 1) + n];
+  pl->dvals.assign(ds.begin(), ds.end());
+  check(cudaMalloc((void **)&pl->d_prefix, sizeof(int) * h.size()), "device allocation");
+  check(cudaMemcpy(pl->d_prefix, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice),
+        "plan upload");
+  for (int s = 0; s < ns; ++s)
+    pl->prefix.push_back(pl->d_prefix + s * (n + 1));
+  Plan &ref = *pl;
+  plans_[active] = std::move(pl);
+  return ref;
+}
+
+int Engine::enqueue(Plan &pl, cudaStream_t s)
+{
+  const int n = (int)pl.active.size();
+  check(cudaMemcpyAsync(d_run_, h_run_, sizeof(JobDesc) * n, cudaMemcpyHostToDevice, s),
+        "descriptor upload");
+  check(cudaMemcpyAsync(d_slot_ptr_, h_slot_ptr_, sizeof(void *) * total_slots_,
+                        cudaMemcpyHostToDevice, s),
+        "slot upload");
+  check(cudaMemcpyAsync(d_slot_T_, h_slot_T_, sizeof(float) * 12 * total_slots_,
+                        cudaMemcpyHostToDevice, s),
+        "slot upload");
+  Batch B;
+  std::memset(&B, 0, sizeof(B));
+  B.jobs = d_run_;
+  B.njobs = n;
+  B.slot_ptr = d_slot_ptr_;
+  B.slot_T = d_slot_T_;
+  const Stages st{params_.bp_levels};
+  return enqueue_range(B, pl.prefix, pl.blocks, params_, pl.dvals, 0, st.count() - 1, s);
+}
+
+void Engine::run(const std::vector<int> &active)
+{
+  if (active.empty())
+    return;
+  check(cudaSetDevice(device_), "cudaSetDevice");
+  Plan &pl = plan_for(active);
+  for (size_t i = 0; i < active.size(); ++i)
+  {
+    const int j = active[i];
+    JobDesc J = master_[j];
+    J.seeds_in = bufs_[j].seeds[seeds_cur_[j]];
+    J.seeds_out = bufs_[j].seeds[seeds_cur_[j] ^ 1];
+    h_run_[i] = J;
+  }
+  if (graphs_)
+  {
+    if (!pl.exec)
+    {
+      cudaGraph_t g = nullptr;
+      check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "graph capture");
+      int nl = 0;
+      try
+      {
+        nl = enqueue(pl, stream_);
+      }
+      catch (...)
+      {
+        cudaStreamEndCapture(stream_, &g);
+        if (g)
+          cudaGraphDestroy(g);
+        throw;
+      }
+      check(cudaStreamEndCapture(stream_, &g), "graph capture");
+      const cudaError_t e = cudaGraphInstantiate(&pl.exec, g, 0);
+      cudaGraphDestroy(g);
+      check(e, "graph instantiate");
+      last_launches_ = nl;
+    }
+    check(cudaEventRecord(ev0_, stream_), "event");
+    check(cudaGraphLaunch(pl.exec, stream_), "graph launch");
+    check(cudaEventRecord(ev1_, stream_), "event");
+  }
+  else
+  {
+    check(cudaEventRecord(ev0_, stream_), "event");
+    last_launches_ = enqueue(pl, stream_);
+    check(cudaEventRecord(ev1_, stream_), "event");
+  }
+  check(cudaStreamSynchronize(stream_), "pipeline run");
+  for (int j : active)
+    seeds_cur_[j] ^= 1;
+}
+
+float Engine::last_run_ms() const
+{
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, ev0_, ev1_);
+  return ms;
+}
+
+void Engine::profile(const std::vector<int> &active, float *ms, int *launches)
+{
+  check(cudaSetDevice(device_), "cudaSetDevice");
+  Plan &pl = plan_for(active);
+  for (size_t i = 0; i < active.size(); ++i)
+  {
+    const int j = active[i];
+    JobDesc J = master_[j];
+    J.seeds_in = bufs_[j].seeds[seeds_cur_[j]];
+    J.seeds_out = bufs_[j].seeds[seeds_cur_[j] ^ 1];
+    h_run_[i] = J;
+  }
+  const int n = (int)pl.active.size();
+  check(cudaMemcpyAsync(d_run_, h_run_, sizeof(JobDesc) * n, cudaMemcpyHostToDevice, stream_),
+        "descriptor upload");
+  check(cudaMemcpyAsync(d_slot_ptr_, h_slot_ptr_, sizeof(void *) * total_slots_,
+                        cudaMemcpyHostToDevice, stream_),
+        "slot upload");
+  check(cudaMemcpyAsync(d_slot_T_, h_slot_T_, sizeof(float) * 12 * total_slots_,
+                        cudaMemcpyHostToDevice, stream_),
+        "slot upload");
+  Batch B;
+  std::memset(&B, 0, sizeof(B));
+  B.jobs = d_run_;
+  B.njobs = n;
+  B.slot_ptr = d_slot_ptr_;
+  B.slot_T = d_slot_T_;
+  const Stages st{params_.bp_levels};
+  LaunchProfile prof;
+  try
+  {
+    enqueue_range(B, pl.prefix, pl.blocks, params_, pl.dvals, 0, st.count() - 1, stream_, &prof);
+    check(cudaStreamSynchronize(stream_), "profile run");
+  }
+  catch (...)
+  {
+    for (auto &m : prof.marks)
+    {
+      cudaEventDestroy(m.e0);
+      cudaEventDestroy(m.e1);
+    }
+    throw;
+  }
+  for (int k = 0; k < kNumKinds; ++k)
+  {
+    ms[k] = 0.0f;
+    launches[k] = 0;
+  }
+  for (auto &m : prof.marks)
+  {
+    float t = 0.0f;
+    cudaEventElapsedTime(&t, m.e0, m.e1);
+    ms[m.kind] += t;
+    launches[m.kind] += 1;
+    cudaEventDestroy(m.e0);
+    cudaEventDestroy(m.e1);
+  }
+  for (int j : active)
+    seeds_cur_[j] ^= 1;
+}
+
+// ---------------------------------------------------------------------------
+// Single-keyframe stage calls (C-ABI stage entry points).
+
+namespace stage
+{
+
+Batch single(const JobDesc &J)
+{
+  Batch B;
+  std::memset(&B, 0, sizeof(B));
+  B.jobs = nullptr;
+  B.njobs = 1;
+  B.one = J;
+  return B;
+}
+
+int run_range(const Batch &B, const Shape &s, const qm_params &p, int first, int last,
+              cudaStream_t stream)
+{
+  const JobLayout lay = JobLayout::make(s, p.bp_levels);
+  const std::vector<int> blocks = stage_blocks(s, lay, p);
+  return enqueue_range(B, {}, blocks, p, {s.D}, first, last, stream);
+}
+
+int first_of(const char *name, int L)
+{
+  const Stages st{L};
+  const std::string n(name);
+  if (n == "quadtree")
+    return st.qt();
+  if (n == "cost")
+    return st.cost();
+  if (n == "bp")
+    return L > 1 ? st.pyr(1) : st.mzero();
+  if (n == "upsample")
+    return st.weights();
+  if (n == "fuse")
+    return st.ftrans();
+  return -1;
+}
+
+int last_of(const char *name, int L)
+{
+  const Stages st{L};
+  const std::string n(name);
+  if (n == "quadtree")
+    return st.qt();
+  if (n == "cost")
+    return st.cost();
+  if (n == "bp")
+    return st.extract();
+  if (n == "upsample")
+    return st.col();
+  if (n == "fuse")
+    return st.fupd();
+  return -1;
+}
+
+} // namespace stage
+
+} // namespace qm

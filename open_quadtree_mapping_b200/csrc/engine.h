@@ -1,0 +1,171 @@
+// Host engine of the dense pipeline: owns the device buffers of N keyframe
+// jobs and runs quadtree -> cost -> BP -> extraction -> upsampling -> fusion
+// for any subset of them, one kernel launch per stage, optionally replayed
+// from a captured CUDA graph.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "launch.h"
+
+namespace qm
+{
+
+// thread-local error message behind qm_last_error()
+void set_error(const std::string &msg);
+const char *get_error();
+
+struct CudaError
+{
+  int status;
+  std::string msg;
+};
+
+// throws CudaError on failure
+void check(cudaError_t e, const char *what);
+
+// Kernel kinds, for per-kind timing (qm_batch_profile).
+enum KernelKind
+{
+  kQuadtree = 0,
+  kCost,
+  kPyramid,
+  kMsgInit,
+  kSweep,
+  kExtract,
+  kWeights,
+  kRowSolve,
+  kColSolve,
+  kFuseTransform,
+  kFuseFill,
+  kFuseUpdate,
+  kNumKinds
+};
+
+struct LaunchProfile
+{
+  struct Mark
+  {
+    int kind;
+    cudaEvent_t e0, e1;
+  };
+  std::vector<Mark> marks;
+};
+
+struct Shape
+{
+  int W, H, D, F;
+  Cam cam;
+};
+
+struct JobBuffers
+{
+  uint8_t *levels = nullptr;
+  float *data[kMaxLevels] = {};
+  float *msg[kMaxLevels][4] = {};
+  int lw[kMaxLevels] = {}, lh[kMaxLevels] = {};
+  int32_t *labels = nullptr;
+  float *sparse = nullptr;
+  float *dense = nullptr;
+  float *row_w = nullptr;
+  float *col_w = nullptr;
+  double *tmp = nullptr;
+  float2 *rowres = nullptr;
+  float4 *seeds[2] = {};
+  unsigned long long *zkey = nullptr;
+  int32_t *table = nullptr;
+};
+
+// Byte layout of one job's buffers (offsets from a 256-byte aligned base).
+struct JobLayout
+{
+  size_t bytes = 0;
+  size_t off_levels, off_data[kMaxLevels], off_msg[kMaxLevels][4], off_labels, off_sparse,
+      off_dense, off_row_w, off_col_w, off_tmp, off_rowres, off_seeds[2], off_zkey, off_table;
+  int lw[kMaxLevels], lh[kMaxLevels];
+  static JobLayout make(const Shape &s, int nlev);
+};
+
+// Fills a JobDesc (geometry, parameters, buffer pointers) for one job.
+JobDesc make_job_desc(const Shape &s, const qm_params &p, const JobBuffers &b, int seeds_cur);
+
+// Validates a parameter struct and a shape; returns an empty string when OK.
+std::string validate(const qm_params &p);
+std::string validate(const Shape &s, const qm_params &p);
+
+KParams kparams(const qm_params &p);
+
+// Stage plan of one active job set: block prefix per stage, in one device
+// buffer, plus the captured graph.
+struct Plan;
+
+class Engine
+{
+public:
+  Engine(int device, const qm_params &p, const std::vector<Shape> &shapes);
+  ~Engine();
+  Engine(const Engine &) = delete;
+  Engine &operator=(const Engine &) = delete;
+
+  int njobs() const { return (int)shapes_.size(); }
+  const Shape &shape(int j) const { return shapes_[j]; }
+  const JobBuffers &buffers(int j) const { return bufs_[j]; }
+  const qm_params &params() const { return params_; }
+  cudaStream_t stream() const { return stream_; }
+  int device() const { return device_; }
+
+  // Inputs of job j for the next run.  Device pointers; T_slot_ref is
+  // F*12 floats (host), T_fuse 12 floats T_income<-lastfuse (host).
+  void set_inputs(int j, const uint8_t *ref, int ref_pitch, const uint8_t *const *slots,
+                  int slot_pitch, const float *T_slot_ref, const float *T_fuse);
+  // Current seed buffer of job j (after the last run).
+  float4 *seeds(int j) const { return bufs_[j].seeds[seeds_cur_[j]]; }
+  void reset_seeds(int j);
+
+  // Runs the pipeline for `active` job indices and waits for it.  Throws
+  // CudaError.  Graph capture is used when `graphs` is set.
+  void run(const std::vector<int> &active);
+  void set_graphs(bool on) { graphs_ = on; }
+  int last_launches() const { return last_launches_; }
+  // Events bracketing the device work of the last run (for timing).
+  float last_run_ms() const;
+  // Runs the pipeline once with eager launches, each bracketed by events;
+  // ms[k] / launches[k] receive the summed device time and launch count per
+  // KernelKind.
+  void profile(const std::vector<int> &active, float *ms, int *launches);
+
+private:
+  Plan &plan_for(const std::vector<int> &active);
+  int enqueue(Plan &pl, cudaStream_t s);
+
+  int device_;
+  qm_params params_;
+  std::vector<Shape> shapes_;
+  std::vector<JobLayout> layouts_;
+  std::vector<JobBuffers> bufs_;
+  std::vector<int> seeds_cur_;
+  void *arena_ = nullptr;
+  // slot tables (all jobs), pinned host + device
+  std::vector<int> slot_base_;
+  int total_slots_ = 0;
+  const uint8_t **h_slot_ptr_ = nullptr;
+  float *h_slot_T_ = nullptr;
+  const uint8_t **d_slot_ptr_ = nullptr;
+  float *d_slot_T_ = nullptr;
+  // job descriptors: host master copy and the packed run arrays
+  std::vector<JobDesc> master_;
+  JobDesc *h_run_ = nullptr;
+  JobDesc *d_run_ = nullptr;
+  cudaStream_t stream_ = nullptr;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  bool graphs_ = true;
+  int last_launches_ = 0;
+  std::map<std::vector<int>, std::unique_ptr<Plan>> plans_;
+};
+
+} // namespace qm

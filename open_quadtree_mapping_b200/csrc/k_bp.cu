@@ -1,0 +1,473 @@
+// Hierarchical min-sum belief propagation and depth extraction
+// (bp_extract and its kernels, bpextract.cu:37-395 of the reference).
+//
+// Layout: per pyramid level, the data cost and the four outgoing-message
+// images are [h][w][D] float arrays (hypotheses contiguous, the PIXEL_COST
+// layout).  A half-sweep updates the cells of one checkerboard colour in
+// place; they only read messages of the other colour, so the update is a
+// Jacobi step inside the colour, exactly as the reference's launch.
+//
+// Warp-per-cell: lane l holds hypotheses l, l+32, l+64, ... of the cell.  The
+// four directions are computed from one load of the data cost and the four
+// incoming messages.  The normalising sum uses the reference's stride-halving
+// tree (bpextract.cu:293-300): strides >= 32 combine register slots, strides
+// 16..1 use __shfl_down, so lane 0 ends with the bit-identical sum.  The
+// argmin of the extraction uses the same tree with the reference's tie rule
+// (the right element wins only when strictly smaller, bpextract.cu:347-355).
+// Hypothesis counts that are not a power of two run the tree over the next
+// power of two with neutral padding (0 for sums, +inf for minima).
+//
+// Bytes per updated cell and half-sweep: 9*D*4 (data + 4 messages read, 4
+// messages written).
+#include <cfloat>
+
+#include "launch.h"
+
+namespace qm
+{
+
+namespace
+{
+
+constexpr __host__ __device__ int pow2_ceil(int n)
+{
+  int p = 1;
+  while (p < n)
+    p <<= 1;
+  return p;
+}
+
+template <int D>
+struct HypLayout
+{
+  static constexpr int NV = (D + 31) / 32; // register slots per lane
+  static constexpr int P = pow2_ceil(D);   // tree width
+};
+
+// Stride-halving tree sum over D values held as v[k] = value(lane + 32k);
+// the result is valid in lane 0.
+template <int D>
+__device__ __forceinline__ float tree_sum(float (&v)[HypLayout<D>::NV])
+{
+  constexpr int P = HypLayout<D>::P;
+  constexpr int NV = HypLayout<D>::NV;
+  float a[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k)
+    a[k] = v[k];
+#pragma unroll
+  for (int s = P / 2; s >= 32; s /= 2)
+  {
+    const int t = s / 32;
+#pragma unroll
+    for (int k = 0; k < t; ++k)
+      if (k + t < NV)
+        a[k] += a[k + t];
+  }
+  float r = a[0];
+#pragma unroll
+  for (int o = (P / 2 < 16 ? P / 2 : 16); o > 0; o >>= 1)
+    r += __shfl_down_sync(0xffffffffu, r, o);
+  return r;
+}
+
+template <int D>
+__device__ __forceinline__ void tree_argmin(const float (&v)[HypLayout<D>::NV], int lane,
+                                            float &best_v, int &best_i)
+{
+  constexpr int P = HypLayout<D>::P;
+  constexpr int NV = HypLayout<D>::NV;
+  float a[NV];
+  int ai[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k)
+  {
+    a[k] = v[k];
+    ai[k] = lane + 32 * k;
+  }
+#pragma unroll
+  for (int s = P / 2; s >= 32; s /= 2)
+  {
+    const int t = s / 32;
+#pragma unroll
+    for (int k = 0; k < t; ++k)
+      if (k + t < NV && a[k + t] < a[k])
+      {
+        a[k] = a[k + t];
+        ai[k] = ai[k + t];
+      }
+  }
+  float r = a[0];
+  int ri = ai[0];
+#pragma unroll
+  for (int o = (P / 2 < 16 ? P / 2 : 16); o > 0; o >>= 1)
+  {
+    const float ov = __shfl_down_sync(0xffffffffu, r, o);
+    const int oi = __shfl_down_sync(0xffffffffu, ri, o);
+    if (ov < r)
+    {
+      r = ov;
+      ri = oi;
+    }
+  }
+  best_v = r;
+  best_i = ri;
+}
+
+// sum / (float)DEPTH_NUM (bpextract.cu:302); D is a compile-time constant
+// here as DEPTH_NUM is in the reference.
+template <int D, int ARITH>
+__device__ __forceinline__ float mean_of(float sum)
+{
+  if (ARITH == QM_ARITH_IEEE)
+    return __fdiv_rn(sum, (float)D);
+  return sum / (float)D;
+}
+
+// ------------------------------------------------------------- pyramid
+// cost_distribute (bpextract.cu:169-198): L_l(x,y) = sum of the existing 2x2
+// children, x offset outer, y offset inner, starting from 0.
+__global__ void __launch_bounds__(kFlatThreads)
+    k_pyramid(const __grid_constant__ Batch B, int level)
+{
+  int lb;
+  const JobDesc &J = job_of(B, lb);
+  const LevelDesc &Lf = J.lv[level - 1];
+  const LevelDesc &Lc = J.lv[level];
+  const int D = J.D;
+  const long t = (long)lb * blockDim.x + threadIdx.x;
+  if (t >= (long)Lc.w * Lc.h * D)
+    return;
+  const int cell = (int)(t / D);
+  const int d = (int)(t - (long)cell * D);
+  const int x = cell % Lc.w, y = cell / Lc.w;
+  float s = 0.0f;
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int jj = 0; jj < 2; ++jj)
+      if (2 * x + i < Lf.w && 2 * y + jj < Lf.h)
+        s += Lf.data[((size_t)(2 * y + jj) * Lf.w + (2 * x + i)) * D + d];
+  Lc.data[(size_t)cell * D + d] = s;
+}
+
+// Messages of the coarsest level start at zero (bpextract.cu:87-90).
+__global__ void __launch_bounds__(kFlatThreads)
+    k_msg_zero(const __grid_constant__ Batch B, int level)
+{
+  int lb;
+  const JobDesc &J = job_of(B, lb);
+  const LevelDesc &L = J.lv[level];
+  const long n = (long)L.w * L.h * J.D;
+  const long t = (long)lb * blockDim.x + threadIdx.x;
+  if (t >= n)
+    return;
+#pragma unroll
+  for (int m = 0; m < 4; ++m)
+    L.msg[m][t] = 0.0f;
+}
+
+// upsample (bpextract.cu:374-395): every cell of level l starts from the
+// message of its parent at level l+1.
+__global__ void __launch_bounds__(kFlatThreads)
+    k_msg_upsample(const __grid_constant__ Batch B, int level)
+{
+  int lb;
+  const JobDesc &J = job_of(B, lb);
+  const LevelDesc &F = J.lv[level];
+  const LevelDesc &C = J.lv[level + 1];
+  const int D = J.D;
+  const long t = (long)lb * blockDim.x + threadIdx.x;
+  if (t >= (long)F.w * F.h * D)
+    return;
+  const int cell = (int)(t / D);
+  const int d = (int)(t - (long)cell * D);
+  const int x = cell % F.w, y = cell / F.w;
+  const size_t src = ((size_t)(y >> 1) * C.w + (x >> 1)) * D + d;
+#pragma unroll
+  for (int m = 0; m < 4; ++m)
+    F.msg[m][t] = C.msg[m][src];
+}
+
+// ------------------------------------------------------------- sweep
+// bp kernel (bpextract.cu:200-312), one warp per cell of the active colour.
+template <int D, int ARITH>
+__global__ void __launch_bounds__(kCellWarps * 32)
+    k_bp_sweep(const __grid_constant__ Batch B, int level, int parity, KParams kp)
+{
+  constexpr int NV = HypLayout<D>::NV;
+  int lb;
+  const JobDesc &J = job_of(B, lb);
+  if (J.D != D)
+    return;
+  const LevelDesc &L = J.lv[level];
+  const int w = L.w, h = L.h, hw = (w + 1) / 2;
+  const int warp = lb * kCellWarps + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (warp >= hw * h)
+    return;
+  const int y = warp / hw, bx = warp - y * hw;
+  // quadtree skip test on the pre-checkerboard column (bpextract.cu:214-220)
+  const int ilev = level + 2;
+  if (ilev <= kp.qt_max)
+  {
+    const int size = 1 << ilev;
+    const int sx = min(bx * size, J.W - 1), sy = min(y * size, J.H - 1);
+    if ((int)J.levels[(size_t)sy * J.W + sx] > ilev)
+      return;
+  }
+  const int x = 2 * bx + ((y + parity) & 1);
+  if (x >= w)
+    return;
+  const bool has_u = y > 0, has_d = y < h - 1, has_l = x > 0, has_r = x < w - 1;
+  const size_t c = (size_t)y * w + x;
+
+  float dat[NV], fu[NV], fd[NV], fl[NV], fr[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k)
+  {
+    const int d = lane + 32 * k;
+    const bool in = d < D;
+    dat[k] = in ? L.data[c * D + d] : 0.0f;
+    fu[k] = (in && has_u) ? L.msg[kDown][(c - w) * D + d] : 0.0f;
+    fd[k] = (in && has_d) ? L.msg[kUp][(c + w) * D + d] : 0.0f;
+    fl[k] = (in && has_l) ? L.msg[kRight][(c - 1) * D + d] : 0.0f;
+    fr[k] = (in && has_r) ? L.msg[kLeft][(c + 1) * D + d] : 0.0f;
+  }
+  const float P1 = kp.P1, P2 = kp.P2;
+#pragma unroll
+  for (int dir = 0; dir < 4; ++dir)
+  {
+    float hv[NV];
+    float lmin = FLT_MAX;
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+    {
+      float v = dat[k];
+      if (dir != kUp && has_u)
+        v += fu[k];
+      if (dir != kDown && has_d)
+        v += fd[k];
+      if (dir != kLeft && has_l)
+        v += fl[k];
+      if (dir != kRight && has_r)
+        v += fr[k];
+      const bool in = lane + 32 * k < D;
+      hv[k] = in ? v : FLT_MAX;
+      lmin = fminf(lmin, hv[k]);
+    }
+    const float hmin = warp_min(lmin);
+    float m[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+    {
+      const int d = lane + 32 * k;
+      float prev = __shfl_up_sync(0xffffffffu, hv[k], 1);
+      float next = __shfl_down_sync(0xffffffffu, hv[k], 1);
+      if (k > 0)
+      {
+        const float wrap = __shfl_sync(0xffffffffu, hv[k > 0 ? k - 1 : 0], 31);
+        if (lane == 0)
+          prev = wrap;
+      }
+      if (k + 1 < NV)
+      {
+        const float wrap = __shfl_sync(0xffffffffu, hv[k + 1 < NV ? k + 1 : k], 0);
+        if (lane == 31)
+          next = wrap;
+      }
+      float mv = hv[k];
+      if (d > 0)
+        mv = fminf(mv, prev + P1);
+      if (d < D - 1)
+        mv = fminf(mv, next + P1);
+      mv = fminf(mv, hmin + P2);
+      m[k] = d < D ? mv : 0.0f;
+    }
+    const float sum = __shfl_sync(0xffffffffu, tree_sum<D>(m), 0);
+    const float mean = mean_of<D, ARITH>(sum);
+    float *out = L.msg[dir] + c * D;
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+    {
+      const int d = lane + 32 * k;
+      if (d < D)
+        out[d] = m[k] - mean;
+    }
+  }
+}
+
+// ------------------------------------------------------------- extract
+// depth_extract (bpextract.cu:314-372), one warp per level-0 cell.
+template <int D, int ARITH>
+__global__ void __launch_bounds__(kCellWarps * 32)
+    k_extract(const __grid_constant__ Batch B)
+{
+  constexpr int NV = HypLayout<D>::NV;
+  int lb;
+  const JobDesc &J = job_of(B, lb);
+  if (J.D != D)
+    return;
+  const LevelDesc &L = J.lv[0];
+  const int w = L.w, h = L.h;
+  const int cell = lb * kCellWarps + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (cell >= w * h)
+    return;
+  const int x = cell % w, y = cell / w;
+  const int lvl = J.levels[(size_t)min(y * 4, J.H - 1) * J.W + min(x * 4, J.W - 1)];
+  const int size = 1 << lvl;
+  if ((x * 4) % size != 0 || (y * 4) % size != 0)
+  {
+    if (lane == 0 && J.labels)
+      J.labels[cell] = -1;
+    return;
+  }
+  const size_t c = (size_t)cell;
+  float b[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k)
+  {
+    const int d = lane + 32 * k;
+    if (d < D)
+    {
+      float v = L.data[c * D + d];
+      if (x != 0)
+        v += L.msg[kRight][(c - 1) * D + d];
+      if (x != w - 1)
+        v += L.msg[kLeft][(c + 1) * D + d];
+      if (y != 0)
+        v += L.msg[kDown][(c - w) * D + d];
+      if (y != h - 1)
+        v += L.msg[kUp][(c + w) * D + d];
+      b[k] = v;
+    }
+    else
+    {
+      b[k] = __int_as_float(0x7f800000); // +inf padding
+    }
+  }
+  float bmin;
+  int best;
+  tree_argmin<D>(b, lane, bmin, best);
+  best = __shfl_sync(0xffffffffu, best, 0);
+  bmin = __shfl_sync(0xffffffffu, bmin, 0);
+  // neighbours of the winner for the parabola
+  const int ip = best > 0 ? best - 1 : 0, in_ = best < D - 1 ? best + 1 : D - 1;
+  float pre = 0.0f, post = 0.0f;
+#pragma unroll
+  for (int k = 0; k < NV; ++k)
+  {
+    const float vp = __shfl_sync(0xffffffffu, b[k], ip & 31);
+    const float vn = __shfl_sync(0xffffffffu, b[k], in_ & 31);
+    if ((ip >> 5) == k)
+      pre = vp;
+    if ((in_ >> 5) == k)
+      post = vn;
+  }
+  if (lane != 0)
+    return;
+  float disparity = (float)best;
+  if (best > 0 && best < D - 1)
+  {
+    if (ARITH == QM_ARITH_IEEE)
+    {
+      const float a = __fadd_rn(__fsub_rn(pre, __fmul_rn(2.0f, bmin)), post);
+      const float bb = __fadd_rn(-pre, post);
+      const float b_a = __fdiv_rn(bb, a);
+      if (isfinite(b_a))
+        disparity = __fsub_rn((float)best, __fdiv_rn(b_a, 2.0f));
+    }
+    else
+    {
+      const float a = pre - 2.0f * bmin + post;
+      const float bb = -pre + post;
+      const float b_a = bb / a;
+      if (isfinite(b_a))
+        disparity = (float)best - b_a / 2.0f;
+    }
+  }
+  float depth;
+  if (ARITH == QM_ARITH_IEEE)
+    depth = (float)__ddiv_rn(1.0, __dadd_rn(__dmul_rn(J.step, (double)disparity), J.min_inv));
+  else
+    depth = 1.0 / (J.step * disparity + J.min_inv);
+  J.sparse[(size_t)(y * 4) * J.W + x * 4] = depth;
+  if (J.labels)
+    J.labels[cell] = best;
+}
+
+template <int D>
+void sweep_d(const Batch &B, int blocks, int level,
+             int parity, KParams kp, int arith, cudaStream_t s)
+{
+  if (arith == QM_ARITH_IEEE)
+    k_bp_sweep<D, QM_ARITH_IEEE><<<blocks, kCellWarps * 32, 0, s>>>(B, level,
+                                                                     parity, kp);
+  else
+    k_bp_sweep<D, QM_ARITH_REFERENCE><<<blocks, kCellWarps * 32, 0, s>>>(B, level, parity, kp);
+}
+
+template <int D>
+void extract_d(const Batch &B, int blocks, int arith,
+               cudaStream_t s)
+{
+  if (arith == QM_ARITH_IEEE)
+    k_extract<D, QM_ARITH_IEEE><<<blocks, kCellWarps * 32, 0, s>>>(B);
+  else
+    k_extract<D, QM_ARITH_REFERENCE><<<blocks, kCellWarps * 32, 0, s>>>(B);
+}
+
+} // namespace
+
+bool bp_supported_d(int d) { return d == 32 || d == 48 || d == 64 || d == 96 || d == 128; }
+
+void launch_pyramid(const Batch &B, int blocks, int level,
+                    cudaStream_t s)
+{
+  k_pyramid<<<blocks, kFlatThreads, 0, s>>>(B, level);
+}
+
+void launch_msg_zero(const Batch &B, int blocks, int level,
+                     cudaStream_t s)
+{
+  k_msg_zero<<<blocks, kFlatThreads, 0, s>>>(B, level);
+}
+
+void launch_msg_upsample(const Batch &B, int blocks, int level,
+                         cudaStream_t s)
+{
+  k_msg_upsample<<<blocks, kFlatThreads, 0, s>>>(B, level);
+}
+
+// A batch with mixed hypothesis counts launches one sweep per count present;
+// each launch skips the jobs of other counts.
+void launch_bp_sweep(const Batch &B, int blocks, int d,
+                     int level, int parity, KParams kp, int arith, cudaStream_t s)
+{
+  switch (d)
+  {
+  case 32: sweep_d<32>(B, blocks, level, parity, kp, arith, s); break;
+  case 48: sweep_d<48>(B, blocks, level, parity, kp, arith, s); break;
+  case 64: sweep_d<64>(B, blocks, level, parity, kp, arith, s); break;
+  case 96: sweep_d<96>(B, blocks, level, parity, kp, arith, s); break;
+  case 128: sweep_d<128>(B, blocks, level, parity, kp, arith, s); break;
+  default: break;
+  }
+}
+
+void launch_extract(const Batch &B, int blocks, int d,
+                    int arith, cudaStream_t s)
+{
+  switch (d)
+  {
+  case 32: extract_d<32>(B, blocks, arith, s); break;
+  case 48: extract_d<48>(B, blocks, arith, s); break;
+  case 64: extract_d<64>(B, blocks, arith, s); break;
+  case 96: extract_d<96>(B, blocks, arith, s); break;
+  case 128: extract_d<128>(B, blocks, arith, s); break;
+  default: break;
+  }
+}
+
+} // namespace qm

@@ -1,0 +1,180 @@
+// Bayesian Gaussian x Beta depth fusion (fuse_transform, hole_filling,
+// fuse_currentmap; depth_fusion.cu:13-213 of the reference).
+//
+// The previous seeds (a, b, mu, sigma^2) are moved into the current frame:
+// good seeds (a >= 0.001, a/(a+b) >= 0.45) have their depth moved along their
+// viewing ray by T_income<-last, sigma^2 += 0.01*depth, and they compete for
+// the pixel they project to.  The reference resolves the competition with a
+// compare-and-swap loop that may give up or read a stale depth, and fills
+// holes first-writer-wins; here both are deterministic:
+//  * z-buffer: atomicMin on the 64-bit key (depth bits << 32 | source index);
+//    depths are positive floats, so the key orders by depth, then by index;
+//  * hole filling reads the resolved keys: an empty pixel takes the nearest
+//    (smallest key) non-empty 3x3 neighbour among the pixels that propagate
+//    (x in [2, W-1), y in [2, H-1)); one pass, no chains.
+// Index 0 is the "empty" table value, so pixel (0, 0) never propagates
+// (as in the reference).  The posterior update (fuse_currentmap) runs in FP64;
+// the emitted depth is mu' when the PRIOR inlier ratio a/(a+b) > 0.6, else -1.
+// The last kernel resets the z-buffer keys for the next frame.
+//
+// Bytes per pixel: transform 16 read + 16 written (+ 8-byte atomic), fill
+// 9*8 read (cached) + 4 written, update 4 + 4 + 16 read, 4 + 16 + 8 written.
+#include "launch.h"
+
+namespace qm
+{
+
+namespace
+{
+
+constexpr unsigned long long kEmpty = ~0ull;
+
+template <class A>
+__global__ void __launch_bounds__(kFlatThreads)
+    k_fuse_transform(const __grid_constant__ Batch B)
+{
+  int lb;
+  const JobDesc &J = job_of(B, lb);
+  const int W = J.W, H = J.H;
+  const int idx = lb * blockDim.x + threadIdx.x;
+  if (idx >= W * H)
+    return;
+  const int x = idx % W, y = idx / W;
+  float4 info = J.seeds_in[idx];
+  // is_badpoint (depth_fusion.cu:25-28)
+  if (info.x < 0.001 || A::div(info.x, info.x + info.y) < 0.45)
+    return;
+  const Cam cam{J.fx, J.fy, J.cx, J.cy};
+  const float3 dir = A::ray((float)x, (float)y, cam);
+  float T[12];
+#pragma unroll
+  for (int k = 0; k < 12; ++k)
+    T[k] = J.Tf[k];
+  const float3 q = A::apply(T, A::scale(dir, info.z));
+  const float nd = A::length(q);
+  if (nd <= 0.5)
+    return;
+  info.z = nd;
+  if (A::kIeee)
+    info.w = (float)__dadd_rn((double)info.w, __dmul_rn((double)nd, 0.01));
+  else
+    info.w += nd * 0.01;
+  const float2 uv = A::project(q, cam);
+  const int tx = trunc_int((double)uv.x + 0.5), ty = trunc_int((double)uv.y + 0.5);
+  if (tx >= W || tx < 0 || ty >= H || ty < 0)
+    return;
+  J.seeds_in[idx] = info;
+  if (idx != 0)
+  {
+    const unsigned long long key =
+        ((unsigned long long)__float_as_uint(nd) << 32) | (unsigned long long)(unsigned)idx;
+    atomicMin(J.zkey + (size_t)ty * W + tx, key);
+  }
+}
+
+__global__ void __launch_bounds__(kFlatThreads)
+    k_fuse_fill(const __grid_constant__ Batch B)
+{
+  int lb;
+  const JobDesc &J = job_of(B, lb);
+  const int W = J.W, H = J.H;
+  const int idx = lb * blockDim.x + threadIdx.x;
+  if (idx >= W * H)
+    return;
+  const int x = idx % W, y = idx / W;
+  unsigned long long key = J.zkey[idx];
+  if (key == kEmpty)
+  {
+    for (int i = -1; i <= 1; ++i)
+      for (int jx = -1; jx <= 1; ++jx)
+      {
+        const int nx = x + jx, ny = y + i;
+        if (nx < 2 || nx >= W - 1 || ny < 2 || ny >= H - 1)
+          continue;
+        const unsigned long long k = J.zkey[(size_t)ny * W + nx];
+        key = k < key ? k : key;
+      }
+  }
+  J.table[idx] = key == kEmpty ? 0 : (int)(unsigned)(key & 0xffffffffull);
+}
+
+__global__ void __launch_bounds__(kFlatThreads)
+    k_fuse_update(const __grid_constant__ Batch B)
+{
+  int lb;
+  const JobDesc &J = job_of(B, lb);
+  const int W = J.W, H = J.H;
+  const int idx = lb * blockDim.x + threadIdx.x;
+  if (idx >= W * H)
+    return;
+  const double dep = (double)J.dense[idx];
+  double unc = fmax(0.5, dep * 0.2);
+  unc *= unc;
+  if (dep <= 0.0)
+    unc = 1e9;
+  const int pre = J.table[idx];
+  double a, b, mu, s2;
+  if (pre > 0)
+  {
+    const float4 s = J.seeds_in[pre];
+    a = s.x;
+    b = s.y;
+    mu = s.z;
+    s2 = s.w;
+  }
+  else
+  {
+    a = 10.0;
+    b = 10.0;
+    mu = dep;
+    s2 = 2500.0;
+  }
+  if ((dep - mu) * (dep - mu) > unc + s2)
+  {
+    a = 10.0;
+    b = 10.0;
+    mu = dep;
+    s2 = 2500.0;
+  }
+  const double var = unc + s2;
+  const double new_sq = unc * s2 / var;
+  const double new_mu = (dep * s2 + mu * unc) / var;
+  const double pdf = exp(-(dep - mu) * (dep - mu) / (2.0 * var)) / sqrt(2.0 * M_PI * var);
+  double c1 = (a / (a + b)) * pdf;
+  double c2 = (b / (a + b)) / 50.0;
+  const double norm = c1 + c2;
+  c1 /= norm;
+  c2 /= norm;
+  const double f = c1 * ((a + 1.0) / (a + b + 1.0)) + c2 * (a / (a + b + 1.0));
+  const double e = c1 * (((a + 1.0) * (a + 2.0)) / ((a + b + 1.0) * (a + b + 2.0))) +
+                   c2 * (a * (a + 1.0) / ((a + b + 1.0) * (a + b + 2.0)));
+  const double mu_p = c1 * new_mu + c2 * mu;
+  const double s2_p = c1 * (new_sq + new_mu * new_mu) + c2 * (s2 + mu * mu) - mu_p * mu_p;
+  const double a_p = (e - f) / (f - e / f);
+  const double b_p = a_p * (1.0 - f) / f;
+  J.dense[idx] = (a / (a + b) > 0.60) ? (float)mu_p : -1.0f;
+  J.seeds_out[idx] = make_float4((float)a_p, (float)b_p, (float)mu_p, (float)s2_p);
+  J.zkey[idx] = kEmpty;
+}
+
+} // namespace
+
+void launch_fuse_transform(const Batch &B, int blocks, int arith, cudaStream_t s)
+{
+  if (arith == QM_ARITH_IEEE)
+    k_fuse_transform<ArithIeee><<<blocks, kFlatThreads, 0, s>>>(B);
+  else
+    k_fuse_transform<ArithRef><<<blocks, kFlatThreads, 0, s>>>(B);
+}
+
+void launch_fuse_fill(const Batch &B, int blocks, cudaStream_t s)
+{
+  k_fuse_fill<<<blocks, kFlatThreads, 0, s>>>(B);
+}
+
+void launch_fuse_update(const Batch &B, int blocks, cudaStream_t s)
+{
+  k_fuse_update<<<blocks, kFlatThreads, 0, s>>>(B);
+}
+
+} // namespace qm

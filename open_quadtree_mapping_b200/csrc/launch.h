@@ -1,0 +1,42 @@
+// Host-side launchers of the pipeline kernels (one launch per stage over all
+// jobs of a batch).  `prefix` is the device copy of the per-job block prefix
+// of that stage and `blocks` its last entry.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "qm_internal.cuh"
+
+namespace qm
+{
+
+// threads per block of the flat per-element kernels
+constexpr int kFlatThreads = 256;
+// warps per block of the warp-per-cell kernels (BP sweep, extraction)
+constexpr int kCellWarps = 8;
+// threads per block of the line solvers (one thread per row / column)
+constexpr int kLineThreads = 64;
+
+int quadtree_tile(int qt_max);
+
+// Every launcher takes the batch by value (the kernels receive it as a
+// __grid_constant__ parameter); B.prefix must point at the stage's prefix.
+void launch_quadtree(const Batch &B, int blocks, KParams kp, cudaStream_t s);
+void launch_cost(const Batch &B, int blocks, int arith, cudaStream_t s);
+void launch_pyramid(const Batch &B, int blocks, int level, cudaStream_t s);
+void launch_msg_zero(const Batch &B, int blocks, int level, cudaStream_t s);
+void launch_msg_upsample(const Batch &B, int blocks, int level, cudaStream_t s);
+void launch_bp_sweep(const Batch &B, int blocks, int d, int level, int parity, KParams kp,
+                     int arith, cudaStream_t s);
+void launch_extract(const Batch &B, int blocks, int d, int arith, cudaStream_t s);
+void launch_weights(const Batch &B, int blocks, KParams kp, int arith, cudaStream_t s);
+void launch_row_solve(const Batch &B, int blocks, KParams kp, cudaStream_t s);
+void launch_col_solve(const Batch &B, int blocks, KParams kp, cudaStream_t s);
+void launch_fuse_transform(const Batch &B, int blocks, int arith, cudaStream_t s);
+void launch_fuse_fill(const Batch &B, int blocks, cudaStream_t s);
+void launch_fuse_update(const Batch &B, int blocks, cudaStream_t s);
+
+// supported hypothesis-count classes of the warp-per-cell kernels
+bool bp_supported_d(int d);
+
+} // namespace qm

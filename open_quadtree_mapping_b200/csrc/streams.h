@@ -1,0 +1,104 @@
+// Camera streams: the frame-selection policy of SeedMatrix::add_frames
+// (seed_matrix.cu:106-209) around the dense pipeline engine.
+#pragma once
+
+#include <deque>
+#include <mutex>
+#include <vector>
+
+#include "engine.h"
+
+namespace qm
+{
+
+// 3x4 row-major float rigid transform with the reference's SE3<float>
+// arithmetic (se3.cuh:91-107 inverse, 179-195 composition).  The operation
+// order is kept because the frame poses feed the cost projections, which
+// are compared bit for bit with the reference.
+struct SE3f
+{
+  float d[12];
+  static SE3f identity();
+  static SE3f from(const float *t12);
+  SE3f inv() const;
+};
+SE3f operator*(const SE3f &l, const SE3f &r);
+
+struct StreamDesc
+{
+  int W, H;
+  Cam cam;
+  int D, F;
+  int ratio; // semi2dense_ratio
+};
+
+class StreamSet
+{
+public:
+  StreamSet(int device, const qm_params &p, const std::vector<StreamDesc> &descs);
+  ~StreamSet();
+
+  int size() const { return (int)st_.size(); }
+  // One frame per stream (imgs[i] host, pitch strides[i]); has_result out.
+  void add_frames(const uint8_t *const *imgs, const size_t *strides, const float *T_curr_world,
+                  int *has_result);
+  // Single-stream form used by the Depthmap facade.
+  int add_frame(int i, const uint8_t *img, size_t stride, const float *T_curr_world);
+  void run_resident();
+  void profile_resident(float *ms, int *launches);
+
+  void get_depth(int i, float *out, size_t stride);
+  void get_debug(int i, float *out, size_t stride);
+  void get_reference(int i, uint8_t *out, size_t stride);
+  void get_T_world_ref(int i, float *T) const;
+  const StreamDesc &desc(int i) const { return st_[i].d; }
+  const float *device_depth(int i) const { return eng_->buffers(i).dense; }
+  Engine &engine() { return *eng_; }
+  std::mutex &mutex() { return mu_; }
+
+private:
+  enum Outcome
+  {
+    kFirst,
+    kSkip,
+    kNoOutput,
+    kOutput
+  };
+  struct RingFrame
+  {
+    int slot;
+    SE3f T; // T_frame<-world
+  };
+  struct State
+  {
+    StreamDesc d;
+    uint8_t *pool = nullptr; // (ring capacity + 2) frames, dense W x H
+    std::vector<int> free_slots;
+    std::deque<RingFrame> ring;
+    int income_slot = -1;
+    SE3f income_T, keyframe_T, fuse_T;
+    int frame_index = 0;
+    bool initialized = false;
+    Outcome outcome = kSkip;
+    std::vector<uint8_t> income_host; // copy of the frame being processed
+    std::vector<uint8_t> ref_host;    // image of the last result
+    SE3f T_world_ref;
+  };
+
+  Outcome begin_frame(int i, const uint8_t *img, size_t stride, const float *T);
+  void end_frame(int i);
+  bool need_add_reference(const State &s) const;
+  bool need_switch_keyframe(const State &s) const;
+  uint8_t *frame_ptr(const State &s, int slot) const
+  {
+    return s.pool + (size_t)slot * s.d.W * s.d.H;
+  }
+
+  int device_;
+  std::vector<State> st_;
+  std::unique_ptr<Engine> eng_;
+  std::vector<int> last_active_;
+  std::mutex mu_;
+};
+
+} // namespace qm

@@ -1,0 +1,219 @@
+"""Python mirror of quadmap::Depthmap (include/quadmap/depthmap.h:31-89).
+
+Same constructor arguments (note the reference's fx, cx, fy, cy order), the
+same add_frames / get* methods, numpy images in and out.  All work happens
+in libqm_b200.so through the C-ABI; undistortion (the reference's host-side
+cv::remap, seed_matrix.cu:85) is applied here when remap maps are given.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .params import Params, QmParamsC
+
+
+def _pose12(T) -> np.ndarray:
+    T = np.asarray(T, dtype=np.float32)
+    if T.shape == (4, 4):
+        T = T[:3, :4]
+    return np.ascontiguousarray(T.reshape(12), dtype=np.float32)
+
+
+def _pparams(params):
+    if params is None:
+        return None
+    if isinstance(params, Params):
+        return QmParamsC.from_params(params)
+    return params
+
+
+class Depthmap:
+    """One camera stream: Depthmap(width, height, fx, cx, fy, cy, remap_1,
+    remap_2, semi2dense_ratio) as in depthmap.h:34-44."""
+
+    def __init__(self, width, height, fx, cx, fy, cy, remap_1=None, remap_2=None,
+                 semi2dense_ratio=1, params: Params | None = None, device: int = 0):
+        L = _lib.lib()
+        self._h = ctypes.c_void_p()
+        pc = _pparams(params)
+        _lib.check(L.qm_depthmap_create(ctypes.byref(self._h), int(width), int(height),
+                                        float(fx), float(cx), float(fy), float(cy),
+                                        int(semi2dense_ratio),
+                                        ctypes.byref(pc) if pc is not None else None,
+                                        int(device)))
+        self.width, self.height = int(width), int(height)
+        self.fx, self.fy, self.cx, self.cy = float(fx), float(fy), float(cx), float(cy)
+        self.remap_1, self.remap_2 = remap_1, remap_2
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            _lib.lib().qm_depthmap_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_frames(self, img_curr: np.ndarray, T_curr_world) -> bool:
+        """Depthmap::add_frames (depthmap.h:46-47): u8 image, world->camera pose."""
+        img = np.asarray(img_curr)
+        if self.remap_1 is not None:
+            import cv2  # host-side undistortion, as the reference's SeedMatrix::input_raw
+            img = cv2.remap(img, self.remap_1, self.remap_2, cv2.INTER_LINEAR,
+                            borderMode=cv2.BORDER_CONSTANT)
+        img = np.ascontiguousarray(img, dtype=np.uint8)
+        if img.shape != (self.height, self.width):
+            raise ValueError("image shape %s != (%d, %d)" % (img.shape, self.height, self.width))
+        T = _pose12(T_curr_world)
+        has = ctypes.c_int(0)
+        _lib.check(_lib.lib().qm_depthmap_add_frame(self._h, img.ctypes.data, img.strides[0],
+                                                    T.ctypes.data, ctypes.byref(has)))
+        return bool(has.value)
+
+    def getDepthmap(self) -> np.ndarray:
+        out = np.empty((self.height, self.width), np.float32)
+        _lib.check(_lib.lib().qm_depthmap_get_depth(self._h, out.ctypes.data, self.width))
+        return out
+
+    def getDebugmap(self) -> np.ndarray:
+        out = np.empty((self.height, self.width), np.float32)
+        _lib.check(_lib.lib().qm_depthmap_get_debug(self._h, out.ctypes.data, self.width))
+        return out
+
+    def getReferenceImage(self) -> np.ndarray:
+        out = np.empty((self.height, self.width), np.uint8)
+        _lib.check(_lib.lib().qm_depthmap_get_reference(self._h, out.ctypes.data, self.width))
+        return out
+
+    def getT_world_ref(self) -> np.ndarray:
+        T = np.empty(12, np.float32)
+        _lib.check(_lib.lib().qm_depthmap_get_T_world_ref(self._h, T.ctypes.data))
+        return T.reshape(3, 4)
+
+    def getFx(self):
+        return self.fx
+
+    def getFy(self):
+        return self.fy
+
+    def getCx(self):
+        return self.cx
+
+    def getCy(self):
+        return self.cy
+
+    def getWidth(self):
+        return self.width
+
+    def getHeight(self):
+        return self.height
+
+
+class BatchDepthmap:
+    """N independent Depthmap streams (possibly of different sizes) whose dense
+    pipelines run batched: one launch per stage over all streams, replayed
+    from a CUDA graph (qm_batch_* in include/qm_capi.h)."""
+
+    def __init__(self, streams, params: Params | None = None, device: int = 0):
+        """streams: list of dicts with width, height, fx, fy, cx, cy and optional
+        num_hyp, num_slots, semi2dense_ratio."""
+        n = len(streams)
+        descs = (_lib.QmStreamDesc * n)()
+        for i, s in enumerate(streams):
+            descs[i].width = int(s["width"])
+            descs[i].height = int(s["height"])
+            descs[i].cam = _lib.QmCamera(float(s["fx"]), float(s["fy"]), float(s["cx"]),
+                                         float(s["cy"]))
+            descs[i].num_hyp = int(s.get("num_hyp", 0))
+            descs[i].num_slots = int(s.get("num_slots", 0))
+            descs[i].semi2dense_ratio = int(s.get("semi2dense_ratio", 1))
+        self.shapes = [(int(s["height"]), int(s["width"])) for s in streams]
+        self._h = ctypes.c_void_p()
+        pc = _pparams(params)
+        _lib.check(_lib.lib().qm_batch_create(ctypes.byref(self._h), n, descs,
+                                              ctypes.byref(pc) if pc is not None else None,
+                                              int(device)))
+        self.n = n
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            _lib.lib().qm_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_frames(self, imgs, poses):
+        """imgs: n u8 arrays (any row pitch, e.g. pinned host views);
+        poses: (n, 12) or n world->camera poses.  Returns n booleans."""
+        n = self.n
+        ptrs = (ctypes.c_void_p * n)()
+        strides = (ctypes.c_size_t * n)()
+        keep = []
+        for i, im in enumerate(imgs):
+            a = np.asarray(im)
+            if a.dtype != np.uint8 or a.shape != self.shapes[i] or a.strides[1] != 1:
+                a = np.ascontiguousarray(a, dtype=np.uint8)
+            keep.append(a)
+            ptrs[i] = a.ctypes.data
+            strides[i] = a.strides[0]
+        T = np.ascontiguousarray(np.stack([_pose12(p) for p in poses]), dtype=np.float32)
+        has = (ctypes.c_int * n)()
+        _lib.check(_lib.lib().qm_batch_add_frames(self._h, ptrs, strides, T.ctypes.data, has))
+        return [bool(h) for h in has]
+
+    def get_depth(self, i, out: np.ndarray | None = None) -> np.ndarray:
+        H, W = self.shapes[i]
+        if out is None:
+            out = np.empty((H, W), np.float32)
+        _lib.check(_lib.lib().qm_batch_get_depth(self._h, i, out.ctypes.data,
+                                                 out.strides[0] // 4))
+        return out
+
+    def get_debug(self, i) -> np.ndarray:
+        H, W = self.shapes[i]
+        out = np.empty((H, W), np.float32)
+        _lib.check(_lib.lib().qm_batch_get_debug(self._h, i, out.ctypes.data, W))
+        return out
+
+    def run_resident(self) -> None:
+        _lib.check(_lib.lib().qm_batch_run_resident(self._h))
+
+    def set_graphs(self, on: bool) -> None:
+        _lib.check(_lib.lib().qm_batch_set_graphs(self._h, 1 if on else 0))
+
+    def last_launches(self) -> int:
+        c = ctypes.c_int()
+        _lib.check(_lib.lib().qm_batch_last_launches(self._h, ctypes.byref(c)))
+        return c.value
+
+    KERNEL_KINDS = ("quadtree", "cost", "pyramid", "msg_init", "bp_sweep", "extract",
+                    "up_weights", "row_solve", "col_solve", "fuse_transform", "fuse_fill",
+                    "fuse_update")
+
+    def stream_ptr(self) -> int:
+        """cudaStream_t the batch's kernels run on (for timing events)."""
+        s = ctypes.c_void_p()
+        _lib.check(_lib.lib().qm_batch_stream(self._h, ctypes.byref(s)))
+        return s.value or 0
+
+    def profile(self):
+        """{kind: (ms, launches)} of one eager resident run (qm_batch_profile)."""
+        n = len(self.KERNEL_KINDS)
+        ms = (ctypes.c_float * n)()
+        cnt = (ctypes.c_int * n)()
+        _lib.check(_lib.lib().qm_batch_profile(self._h, ms, cnt))
+        return {k: (ms[i], cnt[i]) for i, k in enumerate(self.KERNEL_KINDS)}
+
+    def device_depth_ptr(self, i) -> int:
+        p = ctypes.c_void_p()
+        _lib.check(_lib.lib().qm_batch_device_depth(self._h, i, ctypes.byref(p)))
+        return p.value

@@ -1,0 +1,367 @@
+// Test infrastructure only: the reference comparator.
+//
+// This translation unit compiles the reference's own depth-path kernels,
+// unmodified, from the reference source tree (src/quadtree.cu,
+// src/depth_extract.cu, src/bpextract.cu, src/depth_upsample.cu,
+// src/depth_fusion.cu are #included by path; see oracle/Makefile), with the
+// reference's flags (-O3 -use_fast_math) for sm_100a.  Only the legacy texture
+// references are swapped for texture objects (ref_shim/quadmap/
+// texture_memory.cuh) and <opencv2/opencv.hpp> for an empty header.
+//
+// The extern "C" functions below replay the host sequences of
+// SeedMatrix::extract_depth (src/seed_matrix.cu:448-551) and
+// SeedMatrix::fuse_output_depth (src/seed_matrix.cu:553-597) on host buffers,
+// so tests can dump every intermediate (level map, cost volume, final BP
+// messages, sparse depth, upsampled depth, fused depth and seeds) and the
+// bench can time the reference kernels on the same inputs.  Nothing in the
+// product links this library.
+#include <cuda_runtime.h>
+#include <chrono>
+#include <cstring>
+#include <vector>
+
+#include <quadmap/pixel_cost.cuh>
+#include <quadmap/device_image.cuh>
+#include <quadmap/se3.cuh>
+#include <quadmap/camera_model/pinhole_camera.cuh>
+#include <quadmap/match_parameter.cuh>
+#include <quadmap/texture_memory.cuh>
+#include <quadmap/stereo_parameter.cuh>
+
+#include "quadtree.cu"
+#include "depth_extract.cu"
+#include "bpextract.cu"
+#include "depth_upsample.cu"
+#include "depth_fusion.cu"
+
+using namespace quadmap;
+
+namespace
+{
+
+int g_err = 0;
+
+SE3<float> se3_from(const float *t12)
+{
+  SE3<float> s;
+  for (int i = 0; i < 12; ++i)
+    s.data[i] = t12[i];
+  return s;
+}
+
+template <typename T>
+void download(const DeviceImage<T> &img, T *out)
+{
+  if (out)
+    img.getDevData(out);
+}
+
+// The hierarchical BP of bpextract.cu:37-167, replayed kernel for kernel with
+// the same launch shapes, except that the level-0 messages are kept so that
+// the winning labels can be recomputed from them by the caller.
+void bp_keep_messages(DeviceImage<PIXEL_COST> &image_cost_map, float *msg_out)
+{
+  const int width = image_cost_map.width;
+  const int height = image_cost_map.height;
+  const int hbp_level = 4;
+  int hbp_iterate[4] = {4, 10, 10, 10};
+  int h_width[4], h_height[4];
+  h_width[0] = width;
+  h_height[0] = height;
+  for (int i = 1; i < hbp_level; i++)
+  {
+    h_width[i] = (h_width[i - 1] + 1) / 2;
+    h_height[i] = (h_height[i - 1] + 1) / 2;
+  }
+  DeviceImage<PIXEL_COST> *pyr[4];
+  pyr[0] = &image_cost_map;
+  for (int i = 1; i < hbp_level; i++)
+    pyr[i] = new DeviceImage<PIXEL_COST>(h_width[i], h_height[i]);
+  dim3 hb;
+  hb.z = 64;
+  for (int i = 1; i < hbp_level; i++)
+  {
+    dim3 hg(h_width[i], h_height[i]);
+    cost_distribute<<<hg, hb>>>(pyr[i - 1]->dev_ptr, pyr[i]->dev_ptr);
+    cudaDeviceSynchronize();
+  }
+  DeviceImage<PIXEL_COST> *msg[4];
+  for (int m = 0; m < 4; ++m)
+  {
+    msg[m] = new DeviceImage<PIXEL_COST>(h_width[hbp_level - 1], h_height[hbp_level - 1]);
+    msg[m]->zero();
+  }
+  for (int lv = hbp_level - 1; lv >= 0; lv--)
+  {
+    if (lv < hbp_level - 1)
+    {
+      DeviceImage<PIXEL_COST> *next[4];
+      for (int m = 0; m < 4; ++m)
+        next[m] = new DeviceImage<PIXEL_COST>(h_width[lv], h_height[lv]);
+      dim3 ub(64);
+      dim3 ug(h_width[lv + 1], h_height[lv + 1]);
+      for (int m = 0; m < 4; m++)
+        upsample<<<ug, ub>>>(msg[m]->dev_ptr, next[m]->dev_ptr);
+      cudaDeviceSynchronize();
+      for (int m = 0; m < 4; m++)
+      {
+        delete msg[m];
+        msg[m] = next[m];
+      }
+    }
+    dim3 bb(4, 64);
+    dim3 bg((h_width[lv] + 1) / 2, h_height[lv]);
+    bool A_set = true;
+    for (int it = 0; it < hbp_iterate[lv]; it++)
+    {
+      bp<<<bg, bb>>>(pyr[lv]->dev_ptr, msg[0]->dev_ptr, msg[1]->dev_ptr, msg[2]->dev_ptr,
+                     msg[3]->dev_ptr, A_set, lv + 2);
+      A_set = !A_set;
+      cudaDeviceSynchronize();
+    }
+  }
+  // bp() argument order is (data, lm, rm, up, dm): msg[0]=left, msg[1]=right,
+  // msg[2]=up, msg[3]=down.  Dump as up, down, left, right.
+  if (msg_out)
+  {
+    const size_t n = (size_t)width * height * DEPTH_NUM;
+    msg[2]->getDevData(reinterpret_cast<PIXEL_COST *>(msg_out + 0 * n));
+    msg[3]->getDevData(reinterpret_cast<PIXEL_COST *>(msg_out + 1 * n));
+    msg[0]->getDevData(reinterpret_cast<PIXEL_COST *>(msg_out + 2 * n));
+    msg[1]->getDevData(reinterpret_cast<PIXEL_COST *>(msg_out + 3 * n));
+  }
+  for (int i = 1; i < hbp_level; i++)
+    delete pyr[i];
+  for (int m = 0; m < 4; ++m)
+    delete msg[m];
+}
+
+struct ExtractState
+{
+  int w, h;
+  PinholeCamera cam;
+  DeviceImage<float> income;
+  DeviceImage<int> age;
+  std::vector<DeviceImage<float> *> frames;
+  MatchParameter mp;
+  ExtractState(int w_, int h_, const PinholeCamera &c)
+      : w(w_), h(h_), cam(c), income(w_, h_), age(w_, h_)
+  {
+    age.zero();
+  }
+  ~ExtractState()
+  {
+    for (auto *f : frames)
+      delete f;
+    if (mp.is_dev_allocated)
+      cudaFree(mp.dev_ptr);
+  }
+};
+
+// SeedMatrix::extract_depth (seed_matrix.cu:448-551) on the given state;
+// debug_image holds the sparse prior on entry and the BP depths on exit.
+void run_extract(ExtractState &st, int nslots, DeviceImage<float> &debug_image,
+                 DeviceImage<float> &depth_output, int *levels_out, float *cost_out,
+                 float *msg_out)
+{
+  bindTexture(income_image_tex, st.income);
+  st.mp.camera_model = st.cam;
+  st.mp.current_frames = (int)st.frames.size();
+  st.mp.setDevData();
+
+  DeviceImage<int> quadtree_index(st.w, st.h);
+  quadtree_index.zero();
+  dim3 qb(16, 16);
+  dim3 qg((st.w + 15) / 16, (st.h + 15) / 16);
+  quadtree_image_kernal<<<qg, qb>>>(quadtree_index.dev_ptr);
+  cudaDeviceSynchronize();
+  bindTexture(quadtree_tex, quadtree_index, cudaFilterModePoint);
+
+  DeviceImage<PIXEL_COST> image_cost(st.w / 4, st.h / 4);
+  DeviceImage<int> add_num(st.w / 4, st.h / 4);
+  image_cost.zero();
+  add_num.zero();
+  dim3 cb(64, nslots);
+  dim3 cg(st.w / 4, st.h / 4);
+  image_to_cost<<<cg, cb>>>(st.mp.dev_ptr, st.age.dev_ptr, image_cost.dev_ptr, add_num.dev_ptr);
+  dim3 nb(64);
+  normalize_the_cost<<<cg, nb>>>(image_cost.dev_ptr, add_num.dev_ptr);
+  cudaDeviceSynchronize();
+
+  download(quadtree_index, levels_out);
+  if (cost_out)
+    image_cost.getDevData(reinterpret_cast<PIXEL_COST *>(cost_out));
+  if (msg_out)
+  {
+    // Same kernels on a copy of the cost volume, keeping the messages.
+    DeviceImage<PIXEL_COST> cost_copy(st.w / 4, st.h / 4);
+    cost_copy = image_cost;
+    bp_keep_messages(cost_copy, msg_out);
+  }
+  bp_extract(image_cost, debug_image);
+  global_upsample(debug_image, depth_output);
+  cudaDeviceSynchronize();
+
+  cudaUnbindTexture(quadtree_tex);
+  cudaUnbindTexture(income_image_tex);
+}
+
+// SeedMatrix::fuse_output_depth (seed_matrix.cu:553-597).
+void run_fuse(int w, int h, const PinholeCamera &cam, DeviceImage<float> &depth_output,
+              DeviceImage<float4> &seeds, const SE3<float> &last_to_income,
+              DeviceImage<int> *table_keep)
+{
+  DeviceImage<int> transform_table(w, h);
+  DeviceImage<float4> new_seed(w, h);
+  transform_table.zero();
+  dim3 b(16, 16);
+  dim3 g((w + 15) / 16, (h + 15) / 16);
+  fuse_transform<<<g, b>>>(seeds.dev_ptr, transform_table.dev_ptr, last_to_income, cam);
+  hole_filling<<<g, b>>>(transform_table.dev_ptr);
+  fuse_currentmap<<<g, b>>>(transform_table.dev_ptr, depth_output.dev_ptr, seeds.dev_ptr,
+                            new_seed.dev_ptr);
+  seeds = new_seed;
+  cudaDeviceSynchronize();
+  if (table_keep)
+    *table_keep = transform_table;
+}
+
+int status()
+{
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess)
+    return 100 + (int)e;
+  e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return 100 + (int)e;
+  return g_err;
+}
+
+} // namespace
+
+extern "C" {
+
+// Depth extraction as SeedMatrix::extract_depth does it.
+//   income_img  w*h float (values 0..255)
+//   frames_img  nframes*w*h float, ring order (index 0 = most recent)
+//   T_frame_income  nframes*12 floats, row-major 3x4 T_frame<-income
+//   nslots      measurement slots (blockDim.y of image_to_cost; reference 5)
+//   debug_inout w*h: sparse prior in, sparse BP depth out
+// Optional outputs (NULL to skip): levels (w*h int), cost ((w/4)*(h/4)*64),
+// msg (4 x (w/4)*(h/4)*64, order up, down, left, right), dense (w*h).
+int qmref_extract(int w, int h, float fx, float fy, float cx, float cy, const float *income_img,
+                  int nframes, const float *frames_img, const float *T_frame_income, int nslots,
+                  float *debug_inout, int *levels_out, float *cost_out, float *msg_out,
+                  float *dense_out)
+{
+  if (nframes < 1 || nframes > KEYFRAME_NUM || nslots < 1 || nslots > 10)
+    return 1;
+  try
+  {
+    ExtractState st(w, h, PinholeCamera(fx, fy, cx, cy));
+    st.income.setDevData(income_img);
+    for (int i = 0; i < nframes; ++i)
+    {
+      auto *f = new DeviceImage<float>(w, h);
+      f->setDevData(frames_img + (size_t)i * w * h);
+      st.frames.push_back(f);
+      FrameElement e;
+      e.frame_ptr = f->dev_ptr;
+      e.transform = se3_from(T_frame_income + 12 * i);
+      st.mp.framelist_dev[i] = e;
+    }
+    DeviceImage<float> debug_image(w, h), depth_output(w, h);
+    debug_image.setDevData(debug_inout);
+    depth_output.zero();
+    run_extract(st, nslots, debug_image, depth_output, levels_out, cost_out, msg_out);
+    debug_image.getDevData(debug_inout);
+    download(depth_output, dense_out);
+  }
+  catch (const std::exception &)
+  {
+    return 2;
+  }
+  return status();
+}
+
+// Depth fusion as SeedMatrix::fuse_output_depth does it.
+//   depth_inout  w*h: upsampled depth in, fused depth (mu' or -1) out
+//   seeds_inout  w*h*4 (a, b, mu, sigma^2): previous seeds in, new seeds out
+//   T_income_last 12 floats, row-major 3x4 T_income<-lastfuse
+//   table_out    w*h int (transform table after hole filling) or NULL
+int qmref_fuse(int w, int h, float fx, float fy, float cx, float cy, float *depth_inout,
+               float *seeds_inout, const float *T_income_last, int *table_out)
+{
+  try
+  {
+    PinholeCamera cam(fx, fy, cx, cy);
+    DeviceImage<float> depth(w, h);
+    DeviceImage<float4> seeds(w, h);
+    DeviceImage<int> table(w, h);
+    depth.setDevData(depth_inout);
+    seeds.setDevData(reinterpret_cast<const float4 *>(seeds_inout));
+    run_fuse(w, h, cam, depth, seeds, se3_from(T_income_last), &table);
+    depth.getDevData(depth_inout);
+    seeds.getDevData(reinterpret_cast<float4 *>(seeds_inout));
+    download(table, table_out);
+  }
+  catch (const std::exception &)
+  {
+    return 2;
+  }
+  return status();
+}
+
+// Wall-clock time of the reference per-keyframe path (extract_depth then
+// fuse_output_depth, with their per-frame allocations and synchronisations),
+// iters timed repetitions after warmup untimed ones.  Returns ms per frame.
+int qmref_time_frames(int w, int h, float fx, float fy, float cx, float cy,
+                      const float *income_img, int nframes, const float *frames_img,
+                      const float *T_frame_income, int nslots, const float *T_income_last,
+                      int warmup, int iters, double *ms_per_frame)
+{
+  if (nframes < 1 || nframes > KEYFRAME_NUM || nslots < 1 || nslots > 10 || iters < 1)
+    return 1;
+  try
+  {
+    PinholeCamera cam(fx, fy, cx, cy);
+    ExtractState st(w, h, cam);
+    st.income.setDevData(income_img);
+    for (int i = 0; i < nframes; ++i)
+    {
+      auto *f = new DeviceImage<float>(w, h);
+      f->setDevData(frames_img + (size_t)i * w * h);
+      st.frames.push_back(f);
+      FrameElement e;
+      e.frame_ptr = f->dev_ptr;
+      e.transform = se3_from(T_frame_income + 12 * i);
+      st.mp.framelist_dev[i] = e;
+    }
+    DeviceImage<float> debug_image(w, h), depth_output(w, h);
+    DeviceImage<float4> seeds(w, h);
+    seeds.zero();
+    SE3<float> last = se3_from(T_income_last);
+    double total = 0.0;
+    for (int it = 0; it < warmup + iters; ++it)
+    {
+      cudaDeviceSynchronize();
+      auto t0 = std::chrono::steady_clock::now();
+      depth_output.zero();
+      debug_image.zero();
+      run_extract(st, nslots, debug_image, depth_output, nullptr, nullptr, nullptr);
+      run_fuse(w, h, cam, depth_output, seeds, last, nullptr);
+      cudaDeviceSynchronize();
+      auto t1 = std::chrono::steady_clock::now();
+      if (it >= warmup)
+        total += std::chrono::duration<double, std::milli>(t1 - t0).count();
+    }
+    *ms_per_frame = total / iters;
+  }
+  catch (const std::exception &)
+  {
+    return 2;
+  }
+  return status();
+}
+
+} // extern "C"

@@ -1,0 +1,127 @@
+"""GPU tests of the Depthmap facade and the batched multi-stream path, all
+through the C-ABI (libqm_b200.so)."""
+import numpy as np
+import pytest
+
+from conftest import sequence
+from open_quadtree_mapping_b200.params import ARITH_IEEE, Params
+from oracle.policy import PolicyReplay
+
+pytestmark = pytest.mark.gpu
+
+W, H = 160, 128
+F_PX = 460.0 * W / 752.0
+
+
+def _stream_kw(W=W, H=H, f=F_PX, **kw):
+    d = dict(width=W, height=H, fx=f, fy=f, cx=W / 2.0, cy=H / 2.0)
+    d.update(kw)
+    return d
+
+
+def test_facade_matches_oracle_replay(oracle_mod, gpu):
+    """Depthmap over a 16-frame sequence: has_result flags follow the frame
+    policy, the debug map (sparse BP depths) is bit-exact with the oracle in
+    IEEE mode, and the fused depth agrees with an oracle replay."""
+    from open_quadtree_mapping_b200.depthmap import Depthmap
+    imgs, Ts, gts = sequence(1, 16, W, H)
+    p = Params(arith=ARITH_IEEE)  # the reference's hypothesis range
+    dm = Depthmap(W, H, F_PX, W / 2.0, F_PX, H / 2.0, semi2dense_ratio=1, params=p)
+    pol = PolicyReplay(num_slots=5)
+    cam = (F_PX, F_PX, W / 2.0, H / 2.0)
+    seeds = np.zeros((H, W, 4), np.float32)
+    n_dense = 0
+    for i in range(16):
+        has = dm.add_frames(imgs[i], Ts[i])
+        r = pol.add(i, Ts[i])
+        assert has == (r["outcome"] in ("first", "dense")), (i, r["outcome"])
+        if r["outcome"] == "first":
+            assert (dm.getDepthmap() == 0).all()
+            continue
+        if r["outcome"] != "dense":
+            continue
+        n_dense += 1
+        slots = [imgs[k] for k in r["slots"]]
+        o = oracle_mod.extract_depth(imgs[i], slots, r["T_slots"], cam, p)
+        debug = dm.getDebugmap()
+        assert np.array_equal(debug, o["sparse"])
+        dense64 = oracle_mod.upsample(o["sparse"].astype(np.float64), imgs[i], p)
+        fused, new_seeds, _, contested = oracle_mod.fuse(dense64, seeds, r["T_fuse"], cam)
+        seeds = new_seeds.astype(np.float32)
+        depth = dm.getDepthmap()
+        valid = fused > 0
+        assert (depth > 0).mean() == pytest.approx(valid.mean(), abs=2e-3)
+        both = valid & (depth > 0)
+        rel = np.abs(depth[both] - fused[both]) / fused[both]
+        assert np.percentile(rel, 99) < 1e-5, np.percentile(rel, 99)
+        assert np.array_equal(dm.getReferenceImage(), imgs[i])
+        T_wr = dm.getT_world_ref()
+        from oracle.policy import se3_inv
+        assert np.array_equal(T_wr.reshape(12), se3_inv(Ts[i]))
+    assert n_dense >= 3
+
+
+def test_batch_equals_plain_and_graph_equals_eager(gpu):
+    """Three streams run batched (one launch per stage, graph replay) give
+    bit-identical maps to three single-stream runs and to eager launches."""
+    from open_quadtree_mapping_b200.depthmap import BatchDepthmap
+    seqs = [sequence(s, 14, W, H) for s in (2, 3, 4)]
+    p = Params.for_range(64, 0.5, 50.0)
+    batch = BatchDepthmap([_stream_kw()] * 3, params=p)
+    eager = BatchDepthmap([_stream_kw()] * 3, params=p)
+    eager.set_graphs(False)
+    singles = [BatchDepthmap([_stream_kw()], params=p) for _ in range(3)]
+    for i in range(14):
+        imgs = [s[0][i] for s in seqs]
+        poses = [s[1][i] for s in seqs]
+        hb = batch.add_frames(imgs, poses)
+        he = eager.add_frames(imgs, poses)
+        hs = [singles[k].add_frames([imgs[k]], [poses[k]])[0] for k in range(3)]
+        assert hb == he == hs
+        if all(hb) and i > 0:
+            for k in range(3):
+                a = batch.get_depth(k)
+                assert np.array_equal(a, eager.get_depth(k))
+                assert np.array_equal(a, singles[k].get_depth(0))
+                assert np.array_equal(batch.get_debug(k), singles[k].get_debug(0))
+    assert batch.last_launches() > 0
+
+
+def test_uneven_batch_equals_per_stream(gpu):
+    """Streams of different sizes, hypothesis and slot counts in one batch."""
+    from open_quadtree_mapping_b200.depthmap import BatchDepthmap
+    shapes = [(160, 128, 64, 5), (192, 144, 48, 3), (128, 96, 96, 7), (160, 120, 32, 2)]
+    seqs = [sequence(10 + k, 13, w, h) for k, (w, h, _, _) in enumerate(shapes)]
+    p = Params.for_range(64, 0.5, 50.0)
+    descs = [_stream_kw(W=w, H=h, f=460.0 * w / 752.0, num_hyp=d, num_slots=f)
+             for (w, h, d, f) in shapes]
+    batch = BatchDepthmap(descs, params=p)
+    singles = [BatchDepthmap([d], params=p) for d in descs]
+    for i in range(13):
+        imgs = [s[0][i] for s in seqs]
+        poses = [s[1][i] for s in seqs]
+        hb = batch.add_frames(imgs, poses)
+        for k in range(len(shapes)):
+            assert singles[k].add_frames([imgs[k]], [poses[k]])[0] == hb[k]
+    for k in range(len(shapes)):
+        assert np.array_equal(batch.get_depth(k), singles[k].get_depth(0))
+        assert np.array_equal(batch.get_debug(k), singles[k].get_debug(0))
+    batch.run_resident()
+
+
+def test_semi2dense_ratio_and_resident_errors(gpu):
+    from open_quadtree_mapping_b200 import _lib
+    from open_quadtree_mapping_b200.depthmap import BatchDepthmap
+    imgs, Ts, _ = sequence(5, 16, W, H)
+    b = BatchDepthmap([_stream_kw(semi2dense_ratio=3)], params=Params())
+    with pytest.raises(_lib.QmError) as e:
+        b.run_resident()
+    assert e.value.status == _lib.QM_ERR_STATE
+    flags = [b.add_frames([imgs[i]], [Ts[i]])[0] for i in range(16)]
+    assert flags[0]
+    # only multiples of the ratio can produce a depth map
+    for i, f in enumerate(flags[1:], start=2):
+        if i % 3 != 0:
+            assert not f
+    with pytest.raises(_lib.QmError):
+        BatchDepthmap([_stream_kw(W=100)], params=Params())

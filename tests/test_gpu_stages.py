@@ -1,0 +1,164 @@
+"""GPU parity of the stage entry points (through the C-ABI) against the oracle.
+
+IEEE arithmetic mode: levels, costs, final BP messages, labels and sparse
+depths are bit-exact with the fp32 oracle; the upsampled depth (FP64
+elimination on the GPU) is within 1e-5 relative of the fp32 oracle and
+within 2e-6 of the fp64 oracle; the fused depth (FP64 update) within 1e-6 of
+the fp64 oracle.  Reference arithmetic mode (fast-math, the default): levels
+exact, costs/labels agree except at projections within a fast-math error of
+a rounding boundary.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import cam_of, keyframe
+from open_quadtree_mapping_b200.params import ARITH_IEEE, ARITH_REFERENCE, Params
+
+pytestmark = pytest.mark.gpu
+
+UPSAMPLE_RTOL_F32 = 1e-5   # vs the fp32 oracle (the reference's order)
+UPSAMPLE_RTOL_F64 = 2e-6   # vs the fp64 oracle
+FUSE_RTOL_F64 = 1e-6
+
+
+def _gpu_extract(kf, p, gpu, slots=None, T=None):
+    from open_quadtree_mapping_b200 import stages
+    ref = torch.from_numpy(kf.ref).to(gpu)
+    slots = kf.meas if slots is None else slots
+    T = kf.T_meas_ref if T is None else T
+    s = [torch.from_numpy(np.ascontiguousarray(m)).to(gpu) for m in slots]
+    g = stages.extract_depth(ref, s, T, cam_of(kf), p, want_messages=True)
+    torch.cuda.synchronize()
+    return {k: (v.cpu().numpy() if v is not None else None) for k, v in g.items()}
+
+
+CASES = [
+    # W, H, D, F, stream
+    (160, 128, 64, 5, 3),
+    (752, 480, 64, 5, 0),
+    (320, 240, 48, 3, 4),
+    (320, 240, 96, 2, 5),
+    (256, 192, 128, 1, 6),
+    (256, 192, 32, 10, 7),
+]
+
+
+@pytest.mark.parametrize("W,H,D,F,stream", CASES)
+def test_ieee_bit_exact_vs_oracle(W, H, D, F, stream, oracle_mod, gpu):
+    kf = keyframe(stream, W, H, F)
+    p = Params.for_range(D, 0.5, 50.0, arith=ARITH_IEEE)
+    g = _gpu_extract(kf, p, gpu)
+    o = oracle_mod.extract_depth(kf.ref, kf.meas, kf.T_meas_ref, cam_of(kf), p,
+                                 want_messages=True)
+    assert np.array_equal(g["levels"], o["levels"])
+    assert np.array_equal(g["cost"], o["cost"])
+    assert np.array_equal(g["messages"], o["messages"])
+    assert np.array_equal(g["labels"], o["labels"])
+    assert np.array_equal(g["sparse"], o["sparse"])
+    d32 = o["dense"]
+    d64 = oracle_mod.upsample(o["sparse"].astype(np.float64), kf.ref, p)
+    assert np.allclose(g["dense"], d32, rtol=UPSAMPLE_RTOL_F32, atol=0)
+    assert np.allclose(g["dense"], d64, rtol=UPSAMPLE_RTOL_F64, atol=0)
+
+
+@pytest.mark.parametrize("W,H,D,F,stream", CASES[:2])
+def test_reference_mode_agrees_with_oracle(W, H, D, F, stream, oracle_mod, gpu):
+    kf = keyframe(stream, W, H, F)
+    p = Params.for_range(D, 0.5, 50.0, arith=ARITH_REFERENCE)
+    g = _gpu_extract(kf, p, gpu)
+    o = oracle_mod.extract_depth(kf.ref, kf.meas, kf.T_meas_ref, cam_of(kf), p)
+    assert np.array_equal(g["levels"], o["levels"])
+    cost_diff = (g["cost"] != o["cost"]).any(axis=2).mean()
+    assert cost_diff < 0.05, cost_diff
+    node = o["labels"] >= 0
+    assert np.array_equal(g["labels"] >= 0, node)
+    agree = (g["labels"][node] == o["labels"][node]).mean()
+    assert agree > 0.99, agree
+
+
+def test_quadtree_odd_sizes(oracle_mod, gpu):
+    from open_quadtree_mapping_b200 import stages
+    rng = np.random.default_rng(11)
+    for (H, W) in [(1080 // 4, 1920 // 4), (37, 53), (8, 8), (100, 30)]:
+        base = rng.integers(0, 40, (H, W)).astype(np.uint8)
+        img = np.where(rng.random((H, W)) < 0.02, 255, base).astype(np.uint8)
+        for p in (Params(), Params(qt_max_level=5, qt_min_level=0), Params(qt_threshold=3.5)):
+            lv = stages.quadtree(torch.from_numpy(img).to(gpu), p).cpu().numpy()
+            assert np.array_equal(lv, oracle_mod.quadtree(img, p))
+
+
+def test_all_slots_out_of_view_and_identity(oracle_mod, gpu):
+    kf = keyframe(3, 160, 128, 2)
+    p = Params.for_range(64, 0.5, 50.0, arith=ARITH_IEEE)
+    far = np.eye(3, 4, dtype=np.float32)
+    far[0, 3] = 1e4
+    ident = np.eye(3, 4, dtype=np.float32)
+    T = np.stack([far.reshape(12), ident.reshape(12)])
+    g = _gpu_extract(kf, p, gpu, slots=[kf.meas[0], kf.ref], T=T)
+    o = oracle_mod.extract_depth(kf.ref, [kf.meas[0], kf.ref], T, cam_of(kf), p,
+                                 want_messages=True)
+    assert np.array_equal(g["cost"], o["cost"])
+    assert np.array_equal(g["labels"], o["labels"])
+
+
+def test_textureless_image(oracle_mod, gpu):
+    """A flat image: every pixel at the top quadtree level, few nodes."""
+    kf = keyframe(3, 160, 128, 3)
+    flat = np.full_like(kf.ref, 90)
+    p = Params.for_range(64, 0.5, 50.0, arith=ARITH_IEEE)
+    g = _gpu_extract(kf, p, gpu, slots=[flat] * 3)
+    from open_quadtree_mapping_b200 import stages
+    lv = stages.quadtree(torch.from_numpy(flat).to(gpu), p).cpu().numpy()
+    assert (lv == 4).all()
+    assert np.isfinite(g["dense"]).all()
+
+
+def test_fuse_vs_oracle(oracle_mod, gpu):
+    """Two fusion steps on a real keyframe pair: table bit-exact (IEEE
+    transform), fused depth and seeds within FP64 tolerance."""
+    from open_quadtree_mapping_b200 import stages
+    kf = keyframe(3, 160, 128, 3)
+    p = Params.for_range(64, 0.5, 50.0, arith=ARITH_IEEE)
+    cam = cam_of(kf)
+    o = oracle_mod.extract_depth(kf.ref, kf.meas, kf.T_meas_ref, cam, p)
+    dense = o["dense"].astype(np.float32)
+    seeds = np.zeros((128, 160, 4), np.float32)
+    T = np.eye(3, 4, dtype=np.float32).reshape(12)
+    gd, gs_in, gs_out, gt = stages.fuse(torch.from_numpy(dense).to(gpu),
+                                        torch.from_numpy(seeds).to(gpu), T, cam, p)
+    od, os_, ot, oc = oracle_mod.fuse(dense.astype(np.float64), seeds, T, cam)
+    assert np.array_equal(gt.cpu().numpy(), ot)
+    assert np.allclose(gd.cpu().numpy(), od, rtol=FUSE_RTOL_F64)
+    seeds2 = gs_out.cpu().numpy()
+    assert np.allclose(seeds2, os_, rtol=FUSE_RTOL_F64, atol=1e-9)
+    # second step: a small motion, seeds now carry information
+    T2 = np.eye(3, 4, dtype=np.float32)
+    T2[0, 3] = 0.02
+    gd2, _, gs2, gt2 = stages.fuse(torch.from_numpy(dense).to(gpu),
+                                   torch.from_numpy(seeds2).to(gpu), T2.reshape(12), cam, p)
+    od2, os2, ot2, oc2 = oracle_mod.fuse(dense.astype(np.float64), seeds2, T2.reshape(12), cam)
+    assert np.array_equal(gt2.cpu().numpy(), ot2)
+    good = od2 > 0
+    assert good.mean() > 0.3
+    assert np.allclose(gd2.cpu().numpy(), od2, rtol=FUSE_RTOL_F64)
+    assert np.allclose(gs2.cpu().numpy(), os2, rtol=FUSE_RTOL_F64, atol=1e-9)
+
+
+def test_invalid_arguments_are_rejected(gpu):
+    import ctypes
+    from open_quadtree_mapping_b200 import _lib
+    L = _lib.lib()
+    p = _lib.default_params()
+    assert L.qm_quadtree(None, 0, 4, 4, ctypes.byref(p), None, None) == _lib.QM_ERR_INVALID_ARG
+    p.num_hyp = 50
+    buf = torch.zeros(64 * 64, dtype=torch.uint8, device=gpu)
+    assert L.qm_quadtree(ctypes.c_void_p(buf.data_ptr()), 64, 64, 64, ctypes.byref(p),
+                         ctypes.c_void_p(buf.data_ptr()), None) == _lib.QM_ERR_INVALID_ARG
+    assert "num_hyp" in _lib.last_error()
+    p = _lib.default_params()
+    nbytes = ctypes.c_size_t()
+    assert L.qm_bp_workspace_size(64, 64, ctypes.byref(p), ctypes.byref(nbytes)) == 0
+    assert L.qm_bp_extract(ctypes.c_void_p(buf.data_ptr()), 64, 64, ctypes.c_void_p(buf.data_ptr()),
+                           ctypes.byref(p), ctypes.c_void_p(buf.data_ptr()), None, None,
+                           ctypes.c_void_p(buf.data_ptr()), 16, None) == _lib.QM_ERR_WORKSPACE
