@@ -152,10 +152,9 @@ int qm_batch_last_launches(qm_batch *b, int *count);
  * record timing events on it. */
 int qm_batch_stream(qm_batch *b, void **stream);
 /* Kernel kinds reported by qm_batch_profile, in this order. */
-#define QM_NUM_KERNEL_KINDS 12
+#define QM_NUM_KERNEL_KINDS 11
 /* quadtree, cost, pyramid, message init/upsample, bp half-sweep, extraction,
- * upsample weights, row solve, column solve, fuse transform, hole fill,
- * fuse update.  Runs the resident pipeline once with eager launches, each
+ * row solve, column solve, fuse transform, hole fill, fuse update.  Runs the resident pipeline once with eager launches, each
  * bracketed by CUDA events; ms[k] and launches[k] receive the summed device
  * time and the launch count of kind k.  No counterpart in the reference
  * (its printf timers measure CPU clock time, seed_matrix.cu:482-546). */

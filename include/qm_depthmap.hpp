@@ -1,0 +1,154 @@
+// C++ drop-in for quadmap::Depthmap (include/quadmap/depthmap.h:31-89 of
+// open_quadtree_mapping) over the C-ABI of libqm_b200.so.
+//
+// Same constructor argument order (width, height, fx, cx, fy, cy, remap_1,
+// remap_2, semi2dense_ratio), same add_frames / get* methods.  The cv::Mat
+// overloads are compiled when QM_WITH_OPENCV is defined (the ROS node's
+// build); raw-buffer overloads are always available.  Poses accept the
+// reference's SE3<float> (anything with data[0..11] in row-major 3x4 order)
+// or a float[12].  Errors from the library are thrown as quadmap::QmError
+// (the reference throws quadmap::CudaException, cuda_exception.cuh:26-44).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "qm_capi.h"
+
+#ifdef QM_WITH_OPENCV
+#include <opencv2/imgproc/imgproc.hpp>
+#endif
+
+namespace quadmap
+{
+
+struct QmError : public std::runtime_error
+{
+  int status;
+  QmError(int s, const std::string &what) : std::runtime_error(what), status(s) {}
+};
+
+inline void qm_check(int status)
+{
+  if (status != QM_OK)
+    throw QmError(status, std::string("libqm_b200: ") + qm_last_error());
+}
+
+class Depthmap
+{
+public:
+  Depthmap(size_t width, size_t height, float fx, float cx, float fy, float cy,
+           int semi2dense_ratio = 1, const qm_params *params = nullptr, int device = 0)
+      : width_(width), height_(height), fx_(fx), fy_(fy), cx_(cx), cy_(cy)
+  {
+    qm_check(qm_depthmap_create(&h_, (int)width, (int)height, fx, cx, fy, cy, semi2dense_ratio,
+                                params, device));
+    T_world_ref_[0] = T_world_ref_[5] = T_world_ref_[10] = 1.0f;
+  }
+
+#ifdef QM_WITH_OPENCV
+  Depthmap(size_t width, size_t height, float fx, float cx, float fy, float cy, cv::Mat remap_1,
+           cv::Mat remap_2, int semi2dense_ratio)
+      : Depthmap(width, height, fx, cx, fy, cy, semi2dense_ratio)
+  {
+    remap_1_ = remap_1;
+    remap_2_ = remap_2;
+  }
+
+  // Depthmap::add_frames (depthmap.h:46-47): undistorts on the host as
+  // SeedMatrix::input_raw does (seed_matrix.cu:85), then runs the pipeline.
+  template <class SE3T>
+  bool add_frames(const cv::Mat &img_curr, const SE3T &T_curr_world)
+  {
+    cv::Mat und = img_curr;
+    if (!remap_1_.empty())
+      cv::remap(img_curr, und, remap_1_, remap_2_, cv::INTER_LINEAR, cv::BORDER_CONSTANT);
+    float T[12];
+    for (int i = 0; i < 12; ++i)
+      T[i] = T_curr_world.data[i];
+    const bool has = add_frames(und.data, und.step, T);
+    if (has)
+    {
+      depth_out_.create((int)height_, (int)width_);
+      debug_out_.create((int)height_, (int)width_);
+      reference_out_.create((int)height_, (int)width_, CV_8UC1);
+      getDepthmap((float *)depth_out_.data, depth_out_.step / sizeof(float));
+      getDebugmap((float *)debug_out_.data, debug_out_.step / sizeof(float));
+      getReferenceImage(reference_out_.data, reference_out_.step);
+    }
+    return has;
+  }
+  const cv::Mat_<float> getDepthmap() const { return depth_out_; }
+  const cv::Mat_<float> getDebugmap() const { return debug_out_; }
+  const cv::Mat getReferenceImage() const { return reference_out_; }
+#endif
+
+  ~Depthmap()
+  {
+    if (h_)
+      qm_depthmap_destroy(h_);
+  }
+  Depthmap(const Depthmap &) = delete;
+  Depthmap &operator=(const Depthmap &) = delete;
+
+  // Raw-buffer form: u8 image with row pitch `stride` bytes, world->camera pose.
+  bool add_frames(const uint8_t *img, size_t stride, const float T_curr_world[12])
+  {
+    int has = 0;
+    qm_check(qm_depthmap_add_frame(h_, img, stride, T_curr_world, &has));
+    if (has)
+      qm_check(qm_depthmap_get_T_world_ref(h_, T_world_ref_));
+    return has != 0;
+  }
+  void getDepthmap(float *out, size_t stride) const
+  {
+    qm_check(qm_depthmap_get_depth(h_, out, stride));
+  }
+  void getDebugmap(float *out, size_t stride) const
+  {
+    qm_check(qm_depthmap_get_debug(h_, out, stride));
+  }
+  void getReferenceImage(uint8_t *out, size_t stride) const
+  {
+    qm_check(qm_depthmap_get_reference(h_, out, stride));
+  }
+  void getT_world_ref(float T[12]) const
+  {
+    for (int i = 0; i < 12; ++i)
+      T[i] = T_world_ref_[i];
+  }
+  template <class SE3T>
+  SE3T getT_world_ref() const
+  {
+    SE3T s;
+    for (int i = 0; i < 12; ++i)
+      s.data[i] = T_world_ref_[i];
+    return s;
+  }
+
+  float getFx() const { return fx_; }
+  float getFy() const { return fy_; }
+  float getCx() const { return cx_; }
+  float getCy() const { return cy_; }
+  size_t getWidth() const { return width_; }
+  size_t getHeight() const { return height_; }
+  std::mutex &getRefImgMutex() { return ref_img_mutex_; }
+
+private:
+  qm_depthmap *h_ = nullptr;
+  size_t width_, height_;
+  float fx_, fy_, cx_, cy_;
+  float T_world_ref_[12] = {};
+  std::mutex ref_img_mutex_;
+#ifdef QM_WITH_OPENCV
+  cv::Mat remap_1_, remap_2_;
+  cv::Mat_<float> depth_out_, debug_out_;
+  cv::Mat reference_out_;
+#endif
+};
+
+} // namespace quadmap

@@ -104,12 +104,8 @@ size_t bp_workspace(int W, int H, const qm_params &p)
   return o;
 }
 
-size_t upsample_workspace(int W, int H)
-{
-  const size_t P = (size_t)W * H;
-  return align256((size_t)(W + 1) * H * 4) + align256((size_t)W * (H + 1) * 4) +
-         align256(P * 3 * 8) + align256(P * 8);
-}
+// the row-pass result (smoothed depth, smoothed indicator) per pixel
+size_t upsample_workspace(int W, int H) { return align256((size_t)W * H * sizeof(float2)); }
 
 size_t fuse_workspace(int W, int H) { return align256((size_t)W * H * 8); }
 
@@ -436,11 +432,8 @@ int qm_cost_volume(const uint8_t *ref, size_t ref_pitch, int width, int height,
     qm::SlotInline si;
     std::memset(&si, 0, sizeof(si));
     for (int f = 0; f < num_slots; ++f)
-    {
       require(slots[f] != nullptr, "NULL slot image");
-      si.ptr[f] = slots[f];
-      std::memcpy(si.T + 12 * f, T_slot_ref + 12 * f, 12 * sizeof(float));
-    }
+    J.F = qm::dedupe_slots(num_slots, slots, T_slot_ref, si.ptr, si.T, si.w);
     run_stage(J, q, stage_shape(width, height, q, num_slots, cam), "cost", stream, &si);
   });
 }
@@ -516,9 +509,10 @@ int qm_upsample(const float *sparse, const uint8_t *img, size_t img_pitch, int w
     check_stage_size(width, height);
     require(width % 16 == 0 && height % 8 == 0,
             "width must be a multiple of 16 and height of 8");
+    require(width <= qm::kMaxRowLen && height <= qm::kMaxColLen,
+            "upsampling supports at most 4096 x 2048");
     require(sparse && img && dense && img_pitch >= (size_t)width, "bad argument");
     const qm_params q = params_or_default(p);
-    const size_t P = (size_t)width * height;
     if (workspace_bytes < upsample_workspace(width, height) || !workspace)
       throw CudaError{QM_ERR_WORKSPACE, "upsample workspace too small"};
     qm::JobDesc J = base_desc(width, height, q);
@@ -526,15 +520,7 @@ int qm_upsample(const float *sparse, const uint8_t *img, size_t img_pitch, int w
     J.ref_pitch = (int)img_pitch;
     J.sparse = const_cast<float *>(sparse);
     J.dense = dense;
-    char *ws = (char *)workspace;
-    size_t o = 0;
-    J.row_w = (float *)(ws + o);
-    o += align256((size_t)(width + 1) * height * 4);
-    J.col_w = (float *)(ws + o);
-    o += align256((size_t)width * (height + 1) * 4);
-    J.tmp = (double *)(ws + o);
-    o += align256(P * 3 * 8);
-    J.rowres = (float2 *)(ws + o);
+    J.rowres = (float2 *)workspace;
     run_stage(J, q, stage_shape(width, height, q, 1, nullptr), "upsample", stream);
   });
 }

@@ -39,13 +39,12 @@ struct Stages
   int mup(int l) const { return 2 + L + l; } // l = 0..L-2
   int sweep(int l) const { return 1 + 2 * L + l; }
   int extract() const { return 1 + 3 * L; }
-  int weights() const { return 2 + 3 * L; }
-  int row() const { return 3 + 3 * L; }
-  int col() const { return 4 + 3 * L; }
-  int ftrans() const { return 5 + 3 * L; }
-  int ffill() const { return 6 + 3 * L; }
-  int fupd() const { return 7 + 3 * L; }
-  int count() const { return 8 + 3 * L; }
+  int row() const { return 2 + 3 * L; }
+  int col() const { return 3 + 3 * L; }
+  int ftrans() const { return 4 + 3 * L; }
+  int ffill() const { return 5 + 3 * L; }
+  int fupd() const { return 6 + 3 * L; }
+  int count() const { return 7 + 3 * L; }
 };
 
 std::vector<int> stage_blocks(const Shape &s, const JobLayout &lay, const qm_params &p)
@@ -65,9 +64,8 @@ std::vector<int> stage_blocks(const Shape &s, const JobLayout &lay, const qm_par
   for (int l = 0; l < L; ++l)
     b[st.sweep(l)] = cdiv((long)((lay.lw[l] + 1) / 2) * lay.lh[l], kCellWarps);
   b[st.extract()] = cdiv((long)lay.lw[0] * lay.lh[0], kCellWarps);
-  b[st.weights()] = cdiv((long)(s.W + 1) * (s.H + 1), kFlatThreads);
-  b[st.row()] = cdiv(s.H, kLineThreads);
-  b[st.col()] = cdiv(s.W, kLineThreads);
+  b[st.row()] = cdiv(s.H, kRowWarps);
+  b[st.col()] = cdiv(s.W, kColLines);
   b[st.ftrans()] = b[st.ffill()] = b[st.fupd()] = cdiv((long)s.W * s.H, kFlatThreads);
   return b;
 }
@@ -77,8 +75,8 @@ std::vector<int> stage_blocks(const Shape &s, const JobLayout &lay, const qm_par
 // every launch is bracketed by a pair of events recorded on `s`.  Returns the
 // number of kernel launches.
 int enqueue_range(Batch B, const std::vector<const int *> &prefix, const std::vector<int> &blocks,
-                  const qm_params &p, const std::vector<int> &dvals, int first, int last,
-                  cudaStream_t s, LaunchProfile *prof = nullptr)
+                  const qm_params &p, const std::vector<int> &dvals, int max_w, int max_h,
+                  int first, int last, cudaStream_t s, LaunchProfile *prof = nullptr)
 {
   const Stages st{p.bp_levels};
   const int L = p.bp_levels;
@@ -130,12 +128,12 @@ int enqueue_range(Batch B, const std::vector<const int *> &prefix, const std::ve
   if (in(st.extract()))
     for (int d : dvals)
       launch(kExtract, [&] { launch_extract(at(st.extract()), blocks[st.extract()], d, ar, s); });
-  if (in(st.weights()))
-    launch(kWeights, [&] { launch_weights(at(st.weights()), blocks[st.weights()], kp, ar, s); });
   if (in(st.row()))
-    launch(kRowSolve, [&] { launch_row_solve(at(st.row()), blocks[st.row()], kp, s); });
+    launch(kRowSolve,
+           [&] { launch_row_solve(at(st.row()), blocks[st.row()], kp, ar, max_w, s); });
   if (in(st.col()))
-    launch(kColSolve, [&] { launch_col_solve(at(st.col()), blocks[st.col()], kp, s); });
+    launch(kColSolve,
+           [&] { launch_col_solve(at(st.col()), blocks[st.col()], kp, ar, max_h, s); });
   if (in(st.ftrans()))
     launch(kFuseTransform,
            [&] { launch_fuse_transform(at(st.ftrans()), blocks[st.ftrans()], ar, s); });
@@ -175,6 +173,28 @@ KParams kparams(const qm_params &p)
   return k;
 }
 
+int dedupe_slots(int F, const uint8_t *const *ptrs, const float *T, const uint8_t **out_ptrs,
+                 float *out_T, int *out_w)
+{
+  int n = 0;
+  for (int f = 0; f < F; ++f)
+  {
+    int k = 0;
+    while (k < n && !(out_ptrs[k] == ptrs[f] &&
+                      std::memcmp(out_T + 12 * k, T + 12 * f, 12 * sizeof(float)) == 0))
+      ++k;
+    if (k == n)
+    {
+      out_ptrs[n] = ptrs[f];
+      std::memcpy(out_T + 12 * n, T + 12 * f, 12 * sizeof(float));
+      out_w[n] = 0;
+      ++n;
+    }
+    out_w[k] += 1;
+  }
+  return n;
+}
+
 std::string validate(const qm_params &p)
 {
   if (!bp_supported_d(p.num_hyp))
@@ -199,8 +219,8 @@ std::string validate(const qm_params &p)
 
 std::string validate(const Shape &s, const qm_params &p)
 {
-  if (s.W < 16 || s.H < 16 || s.W > 16384 || s.H > 16384)
-    return "image size must be within [16, 16384]";
+  if (s.W < 16 || s.H < 16 || s.W > kMaxRowLen || s.H > kMaxColLen)
+    return "image size must be within [16, 4096] x [16, 2048]";
   if (s.W % 16 != 0 || s.H % 8 != 0)
     return "width must be a multiple of 16 and height of 8 (the upsampler's line chunks)";
   if (!bp_supported_d(s.D))
@@ -242,9 +262,6 @@ JobLayout JobLayout::make(const Shape &s, int nlev)
   L.off_labels = take((size_t)(s.W / 4) * (s.H / 4) * sizeof(int32_t));
   L.off_sparse = take(P * sizeof(float));
   L.off_dense = take(P * sizeof(float));
-  L.off_row_w = take((size_t)(s.W + 1) * s.H * sizeof(float));
-  L.off_col_w = take((size_t)s.W * (s.H + 1) * sizeof(float));
-  L.off_tmp = take(P * 3 * sizeof(double));
   L.off_rowres = take(P * sizeof(float2));
   L.off_seeds[0] = take(P * sizeof(float4));
   L.off_seeds[1] = take(P * sizeof(float4));
@@ -283,9 +300,6 @@ JobDesc make_job_desc(const Shape &s, const qm_params &p, const JobBuffers &b, i
   J.labels = b.labels;
   J.sparse = b.sparse;
   J.dense = b.dense;
-  J.row_w = b.row_w;
-  J.col_w = b.col_w;
-  J.tmp = b.tmp;
   J.rowres = b.rowres;
   J.seeds_in = b.seeds[seeds_cur];
   J.seeds_out = b.seeds[seeds_cur ^ 1];
@@ -303,6 +317,7 @@ struct Plan
   std::vector<const int *> prefix; // per stage, into d_prefix
   std::vector<int> blocks;         // per stage, total
   std::vector<int> dvals;
+  int max_w = 0, max_h = 0; // longest lines of the row / column solves
   cudaGraphExec_t exec = nullptr;
   ~Plan()
   {
@@ -331,6 +346,7 @@ Engine::Engine(int device, const qm_params &p, const std::vector<Shape> &shapes)
   check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
   check(cudaEventCreate(&ev0_), "cudaEventCreate");
   check(cudaEventCreate(&ev1_), "cudaEventCreate");
+  prepare_upsample_kernels();
   const int n = njobs();
   size_t total = 0;
   std::vector<size_t> base(n);
@@ -363,9 +379,6 @@ Engine::Engine(int device, const qm_params &p, const std::vector<Shape> &shapes)
     B.labels = (int32_t *)(b0 + L.off_labels);
     B.sparse = (float *)(b0 + L.off_sparse);
     B.dense = (float *)(b0 + L.off_dense);
-    B.row_w = (float *)(b0 + L.off_row_w);
-    B.col_w = (float *)(b0 + L.off_col_w);
-    B.tmp = (double *)(b0 + L.off_tmp);
     B.rowres = (float2 *)(b0 + L.off_rowres);
     B.seeds[0] = (float4 *)(b0 + L.off_seeds[0]);
     B.seeds[1] = (float4 *)(b0 + L.off_seeds[1]);
@@ -389,10 +402,14 @@ Engine::Engine(int device, const qm_params &p, const std::vector<Shape> &shapes)
         "pinned allocation");
   check(cudaHostAlloc((void **)&h_slot_T_, sizeof(float) * 12 * total_slots_, cudaHostAllocDefault),
         "pinned allocation");
+  check(cudaHostAlloc((void **)&h_slot_w_, sizeof(int) * total_slots_, cudaHostAllocDefault),
+        "pinned allocation");
   std::memset(h_slot_ptr_, 0, sizeof(void *) * total_slots_);
   std::memset(h_slot_T_, 0, sizeof(float) * 12 * total_slots_);
+  std::memset(h_slot_w_, 0, sizeof(int) * total_slots_);
   check(cudaMalloc((void **)&d_slot_ptr_, sizeof(void *) * total_slots_), "device allocation");
   check(cudaMalloc((void **)&d_slot_T_, sizeof(float) * 12 * total_slots_), "device allocation");
+  check(cudaMalloc((void **)&d_slot_w_, sizeof(int) * total_slots_), "device allocation");
   master_.resize(n);
   for (int j = 0; j < n; ++j)
   {
@@ -417,12 +434,16 @@ Engine::~Engine()
     cudaFree(d_slot_ptr_);
   if (d_slot_T_)
     cudaFree(d_slot_T_);
+  if (d_slot_w_)
+    cudaFree(d_slot_w_);
   if (d_run_)
     cudaFree(d_run_);
   if (h_slot_ptr_)
     cudaFreeHost(h_slot_ptr_);
   if (h_slot_T_)
     cudaFreeHost(h_slot_T_);
+  if (h_slot_w_)
+    cudaFreeHost(h_slot_w_);
   if (h_run_)
     cudaFreeHost(h_run_);
   if (ev0_)
@@ -440,11 +461,9 @@ void Engine::set_inputs(int j, const uint8_t *ref, int ref_pitch, const uint8_t 
   J.ref = ref;
   J.ref_pitch = ref_pitch;
   J.slot_pitch = slot_pitch;
-  for (int f = 0; f < shapes_[j].F; ++f)
-  {
-    h_slot_ptr_[slot_base_[j] + f] = slots[f];
-    std::memcpy(h_slot_T_ + 12 * (slot_base_[j] + f), T_slot_ref + 12 * f, 12 * sizeof(float));
-  }
+  const int b = slot_base_[j];
+  J.F = dedupe_slots(shapes_[j].F, slots, T_slot_ref, h_slot_ptr_ + b, h_slot_T_ + 12 * b,
+                     h_slot_w_ + b);
   if (T_fuse)
     std::memcpy(J.Tf, T_fuse, 12 * sizeof(float));
 }
@@ -475,6 +494,8 @@ Plan &Engine::plan_for(const std::vector<int> &active)
   {
     const int j = active[i];
     ds.insert(shapes_[j].D);
+    pl->max_w = std::max(pl->max_w, shapes_[j].W);
+    pl->max_h = std::max(pl->max_h, shapes_[j].H);
     const std::vector<int> b = stage_blocks(shapes_[j], layouts_[j], params_);
     for (int s = 0; s < ns; ++s)
       h[s * (n + 1) + i + 1] = h[s * (n + 1) + i] + b[s];
@@ -492,33 +513,8 @@ Plan &Engine::plan_for(const std::vector<int> &active)
   return ref;
 }
 
-int Engine::enqueue(Plan &pl, cudaStream_t s)
+void Engine::pack(const std::vector<int> &active)
 {
-  const int n = (int)pl.active.size();
-  check(cudaMemcpyAsync(d_run_, h_run_, sizeof(JobDesc) * n, cudaMemcpyHostToDevice, s),
-        "descriptor upload");
-  check(cudaMemcpyAsync(d_slot_ptr_, h_slot_ptr_, sizeof(void *) * total_slots_,
-                        cudaMemcpyHostToDevice, s),
-        "slot upload");
-  check(cudaMemcpyAsync(d_slot_T_, h_slot_T_, sizeof(float) * 12 * total_slots_,
-                        cudaMemcpyHostToDevice, s),
-        "slot upload");
-  Batch B;
-  std::memset(&B, 0, sizeof(B));
-  B.jobs = d_run_;
-  B.njobs = n;
-  B.slot_ptr = d_slot_ptr_;
-  B.slot_T = d_slot_T_;
-  const Stages st{params_.bp_levels};
-  return enqueue_range(B, pl.prefix, pl.blocks, params_, pl.dvals, 0, st.count() - 1, s);
-}
-
-void Engine::run(const std::vector<int> &active)
-{
-  if (active.empty())
-    return;
-  check(cudaSetDevice(device_), "cudaSetDevice");
-  Plan &pl = plan_for(active);
   for (size_t i = 0; i < active.size(); ++i)
   {
     const int j = active[i];
@@ -527,6 +523,46 @@ void Engine::run(const std::vector<int> &active)
     J.seeds_out = bufs_[j].seeds[seeds_cur_[j] ^ 1];
     h_run_[i] = J;
   }
+}
+
+Batch Engine::upload(int n, cudaStream_t s)
+{
+  check(cudaMemcpyAsync(d_run_, h_run_, sizeof(JobDesc) * n, cudaMemcpyHostToDevice, s),
+        "descriptor upload");
+  check(cudaMemcpyAsync(d_slot_ptr_, h_slot_ptr_, sizeof(void *) * total_slots_,
+                        cudaMemcpyHostToDevice, s),
+        "slot upload");
+  check(cudaMemcpyAsync(d_slot_T_, h_slot_T_, sizeof(float) * 12 * total_slots_,
+                        cudaMemcpyHostToDevice, s),
+        "slot upload");
+  check(cudaMemcpyAsync(d_slot_w_, h_slot_w_, sizeof(int) * total_slots_,
+                        cudaMemcpyHostToDevice, s),
+        "slot upload");
+  Batch B;
+  std::memset(&B, 0, sizeof(B));
+  B.jobs = d_run_;
+  B.njobs = n;
+  B.slot_ptr = d_slot_ptr_;
+  B.slot_T = d_slot_T_;
+  B.slot_w = d_slot_w_;
+  return B;
+}
+
+int Engine::enqueue(Plan &pl, cudaStream_t s)
+{
+  const Batch B = upload((int)pl.active.size(), s);
+  const Stages st{params_.bp_levels};
+  return enqueue_range(B, pl.prefix, pl.blocks, params_, pl.dvals, pl.max_w, pl.max_h, 0,
+                       st.count() - 1, s);
+}
+
+void Engine::run(const std::vector<int> &active)
+{
+  if (active.empty())
+    return;
+  check(cudaSetDevice(device_), "cudaSetDevice");
+  Plan &pl = plan_for(active);
+  pack(active);
   if (graphs_)
   {
     if (!pl.exec)
@@ -577,34 +613,14 @@ void Engine::profile(const std::vector<int> &active, float *ms, int *launches)
 {
   check(cudaSetDevice(device_), "cudaSetDevice");
   Plan &pl = plan_for(active);
-  for (size_t i = 0; i < active.size(); ++i)
-  {
-    const int j = active[i];
-    JobDesc J = master_[j];
-    J.seeds_in = bufs_[j].seeds[seeds_cur_[j]];
-    J.seeds_out = bufs_[j].seeds[seeds_cur_[j] ^ 1];
-    h_run_[i] = J;
-  }
-  const int n = (int)pl.active.size();
-  check(cudaMemcpyAsync(d_run_, h_run_, sizeof(JobDesc) * n, cudaMemcpyHostToDevice, stream_),
-        "descriptor upload");
-  check(cudaMemcpyAsync(d_slot_ptr_, h_slot_ptr_, sizeof(void *) * total_slots_,
-                        cudaMemcpyHostToDevice, stream_),
-        "slot upload");
-  check(cudaMemcpyAsync(d_slot_T_, h_slot_T_, sizeof(float) * 12 * total_slots_,
-                        cudaMemcpyHostToDevice, stream_),
-        "slot upload");
-  Batch B;
-  std::memset(&B, 0, sizeof(B));
-  B.jobs = d_run_;
-  B.njobs = n;
-  B.slot_ptr = d_slot_ptr_;
-  B.slot_T = d_slot_T_;
+  pack(active);
+  const Batch B = upload((int)pl.active.size(), stream_);
   const Stages st{params_.bp_levels};
   LaunchProfile prof;
   try
   {
-    enqueue_range(B, pl.prefix, pl.blocks, params_, pl.dvals, 0, st.count() - 1, stream_, &prof);
+    enqueue_range(B, pl.prefix, pl.blocks, params_, pl.dvals, pl.max_w, pl.max_h, 0,
+                  st.count() - 1, stream_, &prof);
     check(cudaStreamSynchronize(stream_), "profile run");
   }
   catch (...)
@@ -655,7 +671,7 @@ int run_range(const Batch &B, const Shape &s, const qm_params &p, int first, int
 {
   const JobLayout lay = JobLayout::make(s, p.bp_levels);
   const std::vector<int> blocks = stage_blocks(s, lay, p);
-  return enqueue_range(B, {}, blocks, p, {s.D}, first, last, stream);
+  return enqueue_range(B, {}, blocks, p, {s.D}, s.W, s.H, first, last, stream);
 }
 
 int first_of(const char *name, int L)
@@ -669,7 +685,7 @@ int first_of(const char *name, int L)
   if (n == "bp")
     return L > 1 ? st.pyr(1) : st.mzero();
   if (n == "upsample")
-    return st.weights();
+    return st.row();
   if (n == "fuse")
     return st.ftrans();
   return -1;

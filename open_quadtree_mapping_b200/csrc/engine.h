@@ -38,7 +38,6 @@ enum KernelKind
   kMsgInit,
   kSweep,
   kExtract,
-  kWeights,
   kRowSolve,
   kColSolve,
   kFuseTransform,
@@ -72,9 +71,6 @@ struct JobBuffers
   int32_t *labels = nullptr;
   float *sparse = nullptr;
   float *dense = nullptr;
-  float *row_w = nullptr;
-  float *col_w = nullptr;
-  double *tmp = nullptr;
   float2 *rowres = nullptr;
   float4 *seeds[2] = {};
   unsigned long long *zkey = nullptr;
@@ -86,7 +82,7 @@ struct JobLayout
 {
   size_t bytes = 0;
   size_t off_levels, off_data[kMaxLevels], off_msg[kMaxLevels][4], off_labels, off_sparse,
-      off_dense, off_row_w, off_col_w, off_tmp, off_rowres, off_seeds[2], off_zkey, off_table;
+      off_dense, off_rowres, off_seeds[2], off_zkey, off_table;
   int lw[kMaxLevels], lh[kMaxLevels];
   static JobLayout make(const Shape &s, int nlev);
 };
@@ -99,6 +95,12 @@ std::string validate(const qm_params &p);
 std::string validate(const Shape &s, const qm_params &p);
 
 KParams kparams(const qm_params &p);
+
+// Merges measurement slots with the same image and pose: writes the unique
+// slots (first-occurrence order) with their multiplicities and returns how
+// many there are.
+int dedupe_slots(int F, const uint8_t *const *ptrs, const float *T, const uint8_t **out_ptrs,
+                 float *out_T, int *out_w);
 
 // Stage plan of one active job set: block prefix per stage, in one device
 // buffer, plus the captured graph.
@@ -141,6 +143,10 @@ public:
 
 private:
   Plan &plan_for(const std::vector<int> &active);
+  // packs the descriptors of `active` into the pinned run array
+  void pack(const std::vector<int> &active);
+  // enqueues the descriptor and slot-table uploads; returns the batch
+  Batch upload(int n, cudaStream_t s);
   int enqueue(Plan &pl, cudaStream_t s);
 
   int device_;
@@ -155,8 +161,10 @@ private:
   int total_slots_ = 0;
   const uint8_t **h_slot_ptr_ = nullptr;
   float *h_slot_T_ = nullptr;
+  int *h_slot_w_ = nullptr;
   const uint8_t **d_slot_ptr_ = nullptr;
   float *d_slot_T_ = nullptr;
+  int *d_slot_w_ = nullptr;
   // job descriptors: host master copy and the packed run arrays
   std::vector<JobDesc> master_;
   JobDesc *h_run_ = nullptr;

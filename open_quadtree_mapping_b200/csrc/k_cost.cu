@@ -11,7 +11,11 @@
 //
 // Cells that are not node origins, or touch the border (x <= 0, y <= 0,
 // x >= W-1, y >= H-1), get cost 0 for every hypothesis, as the reference's
-// zeroed cost image does.  A node with no valid slot gets 100.
+// zeroed cost image does.  A node with no valid slot gets 100.  Every node
+// cost is then divided by the cell's writer count, which in the reference is
+// the number of hypotheses: each hypothesis thread of slot row 0 adds 1 to it
+// (depth_extract.cu:219-228), and normalize_the_cost divides by it
+// (depth_extract.cu:231-244).
 //
 // Bytes per cell: 9 reference pixels + D*F*9 measurement gathers (u8, mostly
 // L1/L2 hits along the epipolar segment) + 4*D written.
@@ -25,7 +29,7 @@ namespace
 
 template <class A>
 __global__ void __launch_bounds__(kFlatThreads)
-    k_cost(const __grid_constant__ Batch B, int add_num)
+    k_cost(const __grid_constant__ Batch B)
 {
   int lb;
   const JobDesc &J = job_of(B, lb);
@@ -62,15 +66,19 @@ __global__ void __launch_bounds__(kFlatThreads)
   int sad = 0, nvalid = 0;
   for (int f = 0; f < J.F; ++f)
   {
+    // generic loads: in single-keyframe calls the poses live in the kernel
+    // parameter, not in global memory
     const float *Tg = slot_pose(B, J.slot_base + f);
     float T[12];
 #pragma unroll
     for (int k = 0; k < 12; ++k)
-      T[k] = __ldg(Tg + k);
+      T[k] = Tg[k];
     const float3 q = A::apply(T, p);
     const float2 uv = A::project(q, cam);
-    const int px = trunc_int((double)uv.x + 0.5);
-    const int py = trunc_int((double)uv.y + 0.5);
+    // (int)(u + 0.5) in double in the reference; round_px is its exact
+    // single-precision equivalent for the ranges these tests accept
+    const int px = round_px(uv.x);
+    const int py = round_px(uv.y);
     if (px >= 2 && px < W - 2 && py >= 2 && py < H - 2)
     {
       const uint8_t *m = slot_image(B, J.slot_base + f);
@@ -83,15 +91,17 @@ __global__ void __launch_bounds__(kFlatThreads)
         {
           // In range for any rotation (|r00| + |r01| <= sqrt(2)); the clamp
           // only guards against non-rigid poses.
-          const int chx = min(max(trunc_int((double)A::patch_coord(uv.x, u2u, ii, v2u, jj) + 0.5), 0), W - 1);
-          const int chy = min(max(trunc_int((double)A::patch_coord(uv.y, u2v, ii, v2v, jj) + 0.5), 0), H - 1);
+          const int chx = min(max(round_px(A::patch_coord(uv.x, u2u, ii, v2u, jj)), 0), W - 1);
+          const int chy = min(max(round_px(A::patch_coord(uv.y, u2v, ii, v2v, jj)), 0), H - 1);
           s += abs(patch[ii + 1][jj + 1] - (int)__ldg(m + (size_t)chy * pitch + chx));
         }
-      sad += s;
-      nvalid += 1;
+      const int wgt = slot_weight(B, J.slot_base + f);
+      sad += wgt * s;
+      nvalid += wgt;
     }
   }
   float c = nvalid > 0 ? A::sad_norm((float)sad, (float)nvalid) : 100.0f;
+  const int add_num = D; // writer count of the cell (see above)
   *out = A::div(c, (float)add_num);
 }
 
@@ -99,12 +109,10 @@ __global__ void __launch_bounds__(kFlatThreads)
 
 void launch_cost(const Batch &B, int blocks, int arith, cudaStream_t s)
 {
-  // normalize_the_cost divides by the number of writers of the cell, always 1
-  const int add_num = 1;
   if (arith == QM_ARITH_IEEE)
-    k_cost<ArithIeee><<<blocks, kFlatThreads, 0, s>>>(B, add_num);
+    k_cost<ArithIeee><<<blocks, kFlatThreads, 0, s>>>(B);
   else
-    k_cost<ArithRef><<<blocks, kFlatThreads, 0, s>>>(B, add_num);
+    k_cost<ArithRef><<<blocks, kFlatThreads, 0, s>>>(B);
 }
 
 } // namespace qm

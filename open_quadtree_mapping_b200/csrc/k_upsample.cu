@@ -4,21 +4,36 @@
 // S(d) / S(1[d > 0]).  L_w is the weighted 1-D Laplacian with
 // w = exp(-(dI)^2 / sigma) between neighbours.
 //
-// Differences from the reference, by design:
-//  * the forward elimination (pivots and eliminated right-hand sides) runs in
-//    FP64, the back substitution too; results are rounded to float between
-//    the row and column passes and at the end (the reference is FP32
-//    throughout with approximate divisions).  Agreement with the reference is
-//    within 1e-5 relative; with the FP64 oracle within a few float ulps.
-//  * the forward coefficients are stored transposed ([x][y] for the row pass)
-//    so that consecutive threads (rows) store consecutive addresses.
-// The weight images keep the reference's edge behaviour: the weight grid
-// spans ceil(W/16)*16 x ceil(H/16)*16 threads, so row_w(W, .) / col_w(., H)
-// are exp(0) = 1 when W / H are not multiples of 16, 0 otherwise
-// (depth_upsample.cu:26-37, 64-93).
+// Design.  The reference solves each line with a serial Thomas sweep, one
+// thread per line (480 threads for the row pass of a 752x480 frame).  Here a
+// WARP solves a line: the line is cut into 32 contiguous segments, one per
+// lane, and every recurrence of the Thomas algorithm is turned into a
+// segment-local composition plus a 5-step warp scan:
+//  * pivots: c'_k = c_k / (b_k - a_k c'_{k-1}) is a Moebius map of c'_{k-1};
+//    a segment composes to a 2x2 matrix product (FP64, rescaled by powers of
+//    two), an exclusive warp scan of the matrices gives every lane its
+//    incoming pivot, and the lane then runs its pivots in FP64;
+//  * forward right-hand sides: d'_k = (r_k - a_k d'_{k-1}) / den_k is affine
+//    in d'_{k-1}; segments compose (FP32) and a warp scan gives the incoming
+//    value;
+//  * back substitution: s_k = d'_k - c'_k s_{k+1} is affine in s_{k+1};
+//    a reverse warp scan gives every lane the value after its segment.
+// FP64 is used for the pivots only; the right-hand sides are FP32, as in the
+// reference.  Differences from the reference's serial FP32 sweep are
+// rounding-level (within 1e-5 relative; closer to the FP64 oracle).
 //
-// Bytes per pixel: weights 1 read (u8) + 8 written; row pass 4+8 read,
-// 24 written and read back, 8 written; column pass 8+4 read, 24+24, 4 written.
+// The weights are computed from the image inside the solver (the reference
+// builds two weight images first, depth_upsample.cu:58-93), keeping its edge
+// behaviour: the closing weight of a line is 0 when the line length is a
+// multiple of 16 and exp(0) = 1 otherwise (depth_upsample.cu:26-37).  Each
+// warp keeps its line in shared memory in a skewed layout (segment j of lane
+// l at l*mp + j, mp odd) so that lane-parallel accesses are conflict-free.
+//
+// Row pass: a block holds kRowWarps rows; loads and stores are coalesced
+// along the row.  Column pass: a block holds a stripe of kColLines columns,
+// loaded and stored cooperatively row by row.
+// Bytes per pixel: row pass 1 (image) + 4 (sparse) read, 8 written; column
+// pass 1 + 8 read, 4 written.
 #include "launch.h"
 
 namespace qm
@@ -27,161 +42,302 @@ namespace qm
 namespace
 {
 
-template <class A>
-__global__ void __launch_bounds__(kFlatThreads)
-    k_weights(const __grid_constant__ Batch B, KParams kp)
+constexpr int kArrays = 6; // w, rd, ri, cp, dd (holds 1/den first), di
+
+__host__ __device__ __forceinline__ int seg_len(int n) { return (n + 31) / 32; }
+__host__ __device__ __forceinline__ int seg_pitch(int n) { return seg_len(n) | 1; }
+// floats of one array of a line of n samples (+1 for the closing weight)
+__host__ __device__ __forceinline__ int line_floats(int n) { return 32 * seg_pitch(n) + 1; }
+
+struct LineBuf
 {
-  int lb;
-  const JobDesc &J = job_of(B, lb);
-  const int W = J.W, H = J.H;
-  const long t = (long)lb * blockDim.x + threadIdx.x;
-  if (t >= (long)(W + 1) * (H + 1))
-    return;
-  const int x = (int)(t % (W + 1)), y = (int)(t / (W + 1));
-  const int gw = (W + 15) / 16 * 16, gh = (H + 15) / 16 * 16;
-  auto I = [&](int xx, int yy) {
-    xx = min(max(xx, 0), W - 1);
-    yy = min(max(yy, 0), H - 1);
-    return (float)J.ref[(size_t)yy * J.ref_pitch + xx];
-  };
-  if (y < H)
+  float *w, *rd, *ri, *cp, *dd, *di;
+  int n, m, mp;
+  __device__ __forceinline__ int pos(int k) const
   {
-    float w = 0.0f;
-    if (x >= 1 && x < gw)
-    {
-      const float diff = I(x, y) - I(x - 1, y);
-      w = A::exp((float)((double)(-diff * diff) / kp.up_sigma));
-    }
-    J.row_w[(size_t)y * (W + 1) + x] = w;
+    const int l = k / m;
+    return l * mp + (k - l * m);
   }
-  if (x < W)
-  {
-    float w = 0.0f;
-    if (y >= 1 && y < gh)
-    {
-      const float diff = I(x, y) - I(x, y - 1);
-      w = A::exp((float)((double)(-diff * diff) / kp.up_sigma));
-    }
-    J.col_w[(size_t)y * W + x] = w;
-  }
+};
+
+__device__ __forceinline__ LineBuf line_buf(float *base, int n)
+{
+  LineBuf b;
+  const int L = line_floats(n);
+  b.w = base;
+  b.rd = base + L;
+  b.ri = base + 2 * L;
+  b.cp = base + 3 * L;
+  b.dd = base + 4 * L;
+  b.di = base + 5 * L;
+  b.n = n;
+  b.m = seg_len(n);
+  b.mp = seg_pitch(n);
+  return b;
 }
 
-// One thread per row.  Row pass of global_upsample (smooth_row,
-// depth_upsample.cu:94-197) over the first W/16*16 samples.
-__global__ void __launch_bounds__(kLineThreads)
-    k_row_solve(const __grid_constant__ Batch B, KParams kp)
+// weight between neighbours with intensities a (current) and b (previous),
+// the reference's expression
+template <class A>
+__device__ __forceinline__ float edge_weight(float a, float b, double sigma)
 {
+  const float diff = a - b;
+  return A::exp((float)((double)(-diff * diff) / sigma));
+}
+
+struct Mat2
+{
+  double a, b, c, d; // [[a, b], [c, d]]
+};
+
+__device__ __forceinline__ Mat2 mul(const Mat2 &L, const Mat2 &R)
+{
+  return Mat2{L.a * R.a + L.b * R.c, L.a * R.b + L.b * R.d, L.c * R.a + L.d * R.c,
+              L.c * R.b + L.d * R.d};
+}
+
+// rescale by a power of two (exact) so the largest entry is in [0.5, 1)
+__device__ __forceinline__ Mat2 renorm(const Mat2 &M)
+{
+  const double mx = fmax(fmax(fabs(M.a), fabs(M.b)), fmax(fabs(M.c), fabs(M.d)));
+  if (!(mx > 0.0))
+    return M;
+  int e;
+  frexp(mx, &e);
+  return Mat2{ldexp(M.a, -e), ldexp(M.b, -e), ldexp(M.c, -e), ldexp(M.d, -e)};
+}
+
+__device__ __forceinline__ Mat2 shfl_up(const Mat2 &M, int off)
+{
+  return Mat2{__shfl_up_sync(0xffffffffu, M.a, off), __shfl_up_sync(0xffffffffu, M.b, off),
+              __shfl_up_sync(0xffffffffu, M.c, off), __shfl_up_sync(0xffffffffu, M.d, off)};
+}
+
+struct Aff
+{
+  float g, hd, hi; // z -> g z + h (two right-hand sides)
+};
+
+// Solves the line held in `b` (w, rd, ri filled) and leaves the solution in
+// dd (depth) and di (indicator).  Whole warp.
+__device__ void solve_line(const LineBuf &b, double lam)
+{
+  const int lane = threadIdx.x & 31;
+  const int s = min(lane * b.m, b.n);
+  const int e = min(s + b.m, b.n);
+  const int base = lane * b.mp; // smem position of element s
+  // -------- pivots: segment Moebius product (apply element s first)
+  Mat2 P{1.0, 0.0, 0.0, 1.0};
+  for (int k = s; k < e; ++k)
+  {
+    const int p = base + (k - s);
+    const double wl = b.w[p];
+    const double wr = b.w[k + 1 < b.n ? b.pos(k + 1) : 32 * b.mp];
+    const double a = -lam * wl, bb = 1.0 + lam * (wl + wr), c = -lam * wr;
+    P = renorm(Mat2{c * P.c, c * P.d, bb * P.c - a * P.a, bb * P.d - a * P.b});
+  }
+  // inclusive scan (later segments on the left), then exclusive
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1)
+  {
+    const Mat2 Q = shfl_up(P, off);
+    if (lane >= off)
+      P = renorm(mul(P, Q));
+  }
+  Mat2 E = shfl_up(P, 1);
+  if (lane == 0)
+    E = Mat2{1.0, 0.0, 0.0, 1.0};
+  double cp = E.b / E.d; // incoming pivot c'_{s-1} (0 for lane 0)
+  // -------- pivots of the segment (FP64), forward RHS composition (FP32)
+  Aff F{1.0f, 0.0f, 0.0f};
+  for (int k = s; k < e; ++k)
+  {
+    const int p = base + (k - s);
+    const double wl = b.w[p];
+    const double wr = b.w[k + 1 < b.n ? b.pos(k + 1) : 32 * b.mp];
+    const double a = -lam * wl, bb = 1.0 + lam * (wl + wr), c = -lam * wr;
+    const double inv = 1.0 / (bb - a * cp);
+    cp = c * inv;
+    b.cp[p] = (float)cp;
+    const float invf = (float)inv;
+    b.dd[p] = invf;
+    // alpha_k = -a_k / den_k, formed the same way in both passes below
+    const float alpha = (float)(lam * wl) * invf;
+    F = Aff{alpha * F.g, alpha * F.hd + b.rd[p] * invf, alpha * F.hi + b.ri[p] * invf};
+  }
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1)
+  {
+    const float g = __shfl_up_sync(0xffffffffu, F.g, off);
+    const float hd = __shfl_up_sync(0xffffffffu, F.hd, off);
+    const float hi = __shfl_up_sync(0xffffffffu, F.hi, off);
+    if (lane >= off)
+      F = Aff{F.g * g, F.g * hd + F.hd, F.g * hi + F.hi};
+  }
+  float dprev = __shfl_up_sync(0xffffffffu, F.hd, 1);
+  float iprev = __shfl_up_sync(0xffffffffu, F.hi, 1);
+  if (lane == 0)
+    dprev = iprev = 0.0f;
+  // -------- forward RHS of the segment, back-substitution composition
+  Aff G{1.0f, 0.0f, 0.0f};
+  for (int k = s; k < e; ++k)
+  {
+    const int p = base + (k - s);
+    const float invf = b.dd[p];
+    const float alpha = (float)(lam * (double)b.w[p]) * invf;
+    dprev = alpha * dprev + b.rd[p] * invf;
+    iprev = alpha * iprev + b.ri[p] * invf;
+    b.dd[p] = dprev;
+    b.di[p] = iprev;
+    const float cpk = b.cp[p];
+    G = Aff{-G.g * cpk, G.g * dprev + G.hd, G.g * iprev + G.hi};
+  }
+  // suffix scan: lane l composes with the segments after it
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1)
+  {
+    const float g = __shfl_down_sync(0xffffffffu, G.g, off);
+    const float hd = __shfl_down_sync(0xffffffffu, G.hd, off);
+    const float hi = __shfl_down_sync(0xffffffffu, G.hi, off);
+    if (lane + off < 32)
+      G = Aff{G.g * g, G.g * hd + G.hd, G.g * hi + G.hi};
+  }
+  float zd = __shfl_down_sync(0xffffffffu, G.hd, 1);
+  float zi = __shfl_down_sync(0xffffffffu, G.hi, 1);
+  if (lane == 31)
+    zd = zi = 0.0f;
+  // -------- back substitution of the segment
+  for (int k = e - 1; k >= s; --k)
+  {
+    const int p = base + (k - s);
+    const float cpk = b.cp[p];
+    zd = b.dd[p] - cpk * zd;
+    zi = b.di[p] - cpk * zi;
+    b.dd[p] = zd;
+    b.di[p] = zi;
+  }
+  __syncwarp();
+}
+
+template <class A>
+__global__ void __launch_bounds__(kRowWarps * 32)
+    k_row_solve(const __grid_constant__ Batch B, KParams kp, int max_n)
+{
+  extern __shared__ float smem[];
   int lb;
   const JobDesc &J = job_of(B, lb);
   const int W = J.W, H = J.H;
-  const int y = lb * blockDim.x + threadIdx.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int y = lb * kRowWarps + warp;
   if (y >= H)
     return;
   const int n = W / 16 * 16;
-  if (n == 0)
-    return;
-  const double lam = kp.up_lambda;
-  const float *wrow = J.row_w + (size_t)y * (W + 1);
+  LineBuf b = line_buf(smem + warp * kArrays * line_floats(max_n), n);
+  const uint8_t *img = J.ref + (size_t)y * J.ref_pitch;
   const float *sp = J.sparse + (size_t)y * W;
-  double *tc = J.tmp, *td = J.tmp + (size_t)W * H, *ti = J.tmp + 2 * (size_t)W * H;
-  double fc = 0.0, fd = 0.0, fi = 0.0;
-  double wl = 0.0;
-  for (int x = 0; x < n; ++x)
+  for (int k = lane; k < n; k += 32)
   {
-    const double wr = (double)wrow[x + 1];
-    const float dep = sp[x];
-    const double ind = dep > 0.0f ? 1.0 : 0.0;
-    const double a = -lam * wl;
-    const double b = 1.0 + lam * (wl + wr);
-    const double c = -lam * wr;
-    const double inv = 1.0 / (b - fc * a);
-    fc = c * inv;
-    fd = ((double)dep - fd * a) * inv;
-    fi = (ind - fi * a) * inv;
-    const size_t o = (size_t)x * H + y;
-    tc[o] = fc;
-    td[o] = fd;
-    ti[o] = fi;
-    wl = wr;
+    const int p = b.pos(k);
+    const float I = (float)img[k];
+    b.w[p] = k == 0 ? 0.0f : edge_weight<A>(I, (float)img[k - 1], kp.up_sigma);
+    const float d = sp[k];
+    b.rd[p] = d;
+    b.ri[p] = d > 0.0f ? 1.0f : 0.0f;
   }
-  double nd = 0.0, ni = 0.0;
-  for (int x = n - 1; x >= 0; --x)
+  if (lane == 0)
+    b.w[32 * b.mp] = (n < W) ? edge_weight<A>((float)img[n], (float)img[n - 1], kp.up_sigma)
+                             : (W % 16 != 0 ? 1.0f : 0.0f);
+  __syncwarp();
+  solve_line(b, kp.up_lambda);
+  float2 *out = J.rowres + (size_t)y * W;
+  for (int k = lane; k < n; k += 32)
   {
-    const size_t o = (size_t)x * H + y;
-    const double cc = tc[o];
-    nd = td[o] - cc * nd;
-    ni = ti[o] - cc * ni;
-    J.rowres[(size_t)y * W + x] = make_float2((float)nd, (float)ni);
+    const int p = b.pos(k);
+    out[k] = make_float2(b.dd[p], b.di[p]);
   }
 }
 
-// One thread per column.  Column pass (smooth_col, depth_upsample.cu:198-302)
-// over the first H/8*8 rows, writing S(d)/S(ind).
-__global__ void __launch_bounds__(kLineThreads)
-    k_col_solve(const __grid_constant__ Batch B, KParams kp)
+template <class A>
+__global__ void __launch_bounds__(kColLines * 32)
+    k_col_solve(const __grid_constant__ Batch B, KParams kp, int max_n)
 {
+  extern __shared__ float smem[];
   int lb;
   const JobDesc &J = job_of(B, lb);
   const int W = J.W, H = J.H;
-  const int x = lb * blockDim.x + threadIdx.x;
-  if (x >= W)
-    return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int x0 = lb * kColLines;
   const int n = H / 8 * 8;
-  if (n == 0)
-    return;
-  const double lam = kp.up_lambda;
-  double *tc = J.tmp, *td = J.tmp + (size_t)W * H, *ti = J.tmp + 2 * (size_t)W * H;
-  double fc = 0.0, fd = 0.0, fi = 0.0;
-  double wl = 0.0;
-  for (int y = 0; y < n; ++y)
+  const int per_line = kArrays * line_floats(max_n);
+  // cooperative stripe load: row k, column x0 + c
+  for (int t = threadIdx.x; t < n * kColLines; t += blockDim.x)
   {
-    const double wr = (double)J.col_w[(size_t)(y + 1) * W + x];
-    const float2 r = J.rowres[(size_t)y * W + x];
-    const double a = -lam * wl;
-    const double b = 1.0 + lam * (wl + wr);
-    const double c = -lam * wr;
-    const double inv = 1.0 / (b - fc * a);
-    fc = c * inv;
-    fd = ((double)r.x - fd * a) * inv;
-    fi = ((double)r.y - fi * a) * inv;
-    const size_t o = (size_t)y * W + x;
-    tc[o] = fc;
-    td[o] = fd;
-    ti[o] = fi;
-    wl = wr;
+    const int k = t / kColLines, c = t - k * kColLines;
+    const int x = x0 + c;
+    if (x >= W)
+      continue;
+    LineBuf b = line_buf(smem + c * per_line, n);
+    const int p = b.pos(k);
+    const float2 r = J.rowres[(size_t)k * W + x];
+    b.rd[p] = r.x;
+    b.ri[p] = r.y;
+    const float I = (float)J.ref[(size_t)k * J.ref_pitch + x];
+    b.w[p] = k == 0 ? 0.0f
+                    : edge_weight<A>(I, (float)J.ref[(size_t)(k - 1) * J.ref_pitch + x],
+                                     kp.up_sigma);
+    if (k == n - 1)
+      b.w[32 * b.mp] =
+          (n < H) ? edge_weight<A>((float)J.ref[(size_t)n * J.ref_pitch + x], I, kp.up_sigma)
+                  : (H % 16 != 0 ? 1.0f : 0.0f);
   }
-  double nd = 0.0, ni = 0.0;
-  for (int y = n - 1; y >= 0; --y)
+  __syncthreads();
+  if (x0 + warp < W)
+    solve_line(line_buf(smem + warp * per_line, n), kp.up_lambda);
+  __syncthreads();
+  for (int t = threadIdx.x; t < n * kColLines; t += blockDim.x)
   {
-    const size_t o = (size_t)y * W + x;
-    const double cc = tc[o];
-    nd = td[o] - cc * nd;
-    ni = ti[o] - cc * ni;
-    J.dense[o] = (float)(nd / ni);
+    const int k = t / kColLines, c = t - k * kColLines;
+    const int x = x0 + c;
+    if (x >= W)
+      continue;
+    LineBuf b = line_buf(smem + c * per_line, n);
+    const int p = b.pos(k);
+    J.dense[(size_t)k * W + x] = A::div(b.dd[p], b.di[p]);
   }
 }
 
 } // namespace
 
-void launch_weights(const Batch &B, int blocks, KParams kp,
-                    int arith, cudaStream_t s)
+size_t row_solve_smem(int max_w) { return sizeof(float) * kRowWarps * kArrays * line_floats(max_w); }
+size_t col_solve_smem(int max_h) { return sizeof(float) * kColLines * kArrays * line_floats(max_h); }
+
+void prepare_upsample_kernels()
 {
+  const int mx = 227 * 1024;
+  cudaFuncSetAttribute(k_row_solve<ArithRef>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_row_solve<ArithIeee>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_col_solve<ArithRef>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_col_solve<ArithIeee>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+}
+
+void launch_row_solve(const Batch &B, int blocks, KParams kp, int arith, int max_w,
+                      cudaStream_t s)
+{
+  const size_t sm = row_solve_smem(max_w);
   if (arith == QM_ARITH_IEEE)
-    k_weights<ArithIeee><<<blocks, kFlatThreads, 0, s>>>(B, kp);
+    k_row_solve<ArithIeee><<<blocks, kRowWarps * 32, sm, s>>>(B, kp, max_w);
   else
-    k_weights<ArithRef><<<blocks, kFlatThreads, 0, s>>>(B, kp);
+    k_row_solve<ArithRef><<<blocks, kRowWarps * 32, sm, s>>>(B, kp, max_w);
 }
 
-void launch_row_solve(const Batch &B, int blocks, KParams kp,
+void launch_col_solve(const Batch &B, int blocks, KParams kp, int arith, int max_h,
                       cudaStream_t s)
 {
-  k_row_solve<<<blocks, kLineThreads, 0, s>>>(B, kp);
-}
-
-void launch_col_solve(const Batch &B, int blocks, KParams kp,
-                      cudaStream_t s)
-{
-  k_col_solve<<<blocks, kLineThreads, 0, s>>>(B, kp);
+  const size_t sm = col_solve_smem(max_h);
+  if (arith == QM_ARITH_IEEE)
+    k_col_solve<ArithIeee><<<blocks, kColLines * 32, sm, s>>>(B, kp, max_h);
+  else
+    k_col_solve<ArithRef><<<blocks, kColLines * 32, sm, s>>>(B, kp, max_h);
 }
 
 } // namespace qm

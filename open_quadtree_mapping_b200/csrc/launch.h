@@ -14,8 +14,16 @@ namespace qm
 constexpr int kFlatThreads = 256;
 // warps per block of the warp-per-cell kernels (BP sweep, extraction)
 constexpr int kCellWarps = 8;
-// threads per block of the line solvers (one thread per row / column)
-constexpr int kLineThreads = 64;
+// line solvers: one warp per line; rows per block of the row pass and
+// columns per block (stripe width) of the column pass
+constexpr int kRowWarps = 2;
+constexpr int kColLines = 4;
+// longest lines the solvers' shared memory holds
+constexpr int kMaxRowLen = 4096;
+constexpr int kMaxColLen = 2048;
+size_t row_solve_smem(int max_w);
+size_t col_solve_smem(int max_h);
+void prepare_upsample_kernels();
 
 int quadtree_tile(int qt_max);
 
@@ -29,9 +37,10 @@ void launch_msg_upsample(const Batch &B, int blocks, int level, cudaStream_t s);
 void launch_bp_sweep(const Batch &B, int blocks, int d, int level, int parity, KParams kp,
                      int arith, cudaStream_t s);
 void launch_extract(const Batch &B, int blocks, int d, int arith, cudaStream_t s);
-void launch_weights(const Batch &B, int blocks, KParams kp, int arith, cudaStream_t s);
-void launch_row_solve(const Batch &B, int blocks, KParams kp, cudaStream_t s);
-void launch_col_solve(const Batch &B, int blocks, KParams kp, cudaStream_t s);
+void launch_row_solve(const Batch &B, int blocks, KParams kp, int arith, int max_w,
+                      cudaStream_t s);
+void launch_col_solve(const Batch &B, int blocks, KParams kp, int arith, int max_h,
+                      cudaStream_t s);
 void launch_fuse_transform(const Batch &B, int blocks, int arith, cudaStream_t s);
 void launch_fuse_fill(const Batch &B, int blocks, cudaStream_t s);
 void launch_fuse_update(const Batch &B, int blocks, cudaStream_t s);

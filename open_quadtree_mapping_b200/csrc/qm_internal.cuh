@@ -64,9 +64,6 @@ struct JobDesc
   int32_t *labels; // cw*ch or null
   float *sparse;   // W*H sparse depth (the reference's debug image)
   float *dense;    // W*H upsampled depth, fused in place
-  float *row_w;    // (W+1)*H
-  float *col_w;    // W*(H+1)
-  double *tmp;     // 3*W*H forward-elimination coefficients
   float2 *rowres;  // W*H row-smoothed (depth, indicator)
   float4 *seeds_in;
   float4 *seeds_out;
@@ -79,10 +76,15 @@ struct JobDesc
 // block prefix and the slot tables in device memory; single-keyframe stage
 // calls carry their one job (and its slots) inline in the kernel parameter,
 // so those calls need no device allocation.
+// Measurement slots of a job after merging duplicates: a slot that appears
+// k times (same image, same pose) is evaluated once with weight k.  The SAD
+// and the valid count are integers, so the weighted sums equal the
+// reference's per-slot sums exactly.
 struct SlotInline
 {
   const uint8_t *ptr[kMaxSlots];
   float T[kMaxSlots * 12];
+  int w[kMaxSlots];
 };
 
 struct Batch
@@ -92,6 +94,7 @@ struct Batch
   int njobs;
   const uint8_t *const *slot_ptr; // per slot, device image (null: `slots`)
   const float *slot_T;            // per slot, 12 floats T_slot<-ref
+  const int *slot_w;              // per slot, multiplicity
   JobDesc one;
   SlotInline slots;
 };
@@ -142,9 +145,34 @@ __device__ __forceinline__ const float *slot_pose(const Batch &B, int slot)
   return B.slot_ptr ? B.slot_T + 12 * slot : B.slots.T + 12 * slot;
 }
 
+__device__ __forceinline__ int slot_weight(const Batch &B, int slot)
+{
+  return B.slot_ptr ? B.slot_w[slot] : B.slots.w[slot];
+}
+
 // Double -> int by truncation toward zero with saturation (C conversion as
 // the reference performs it on `float + 0.5`).
 __device__ __forceinline__ int trunc_int(double v) { return (int)v; }
+
+// (int)((double)u + 0.5) -- the reference's pixel rounding -- with
+// single-precision operations only, for callers that only use results >= 0
+// (every result below 0 is reported as -1).  Exact: for 0 <= u < 2^22,
+// adding 2^23 with round-down gives 2^23 + floor(u) exactly, floor(u) and the
+// fraction u - floor(u) are exact, and trunc(u + 0.5) = floor(u) + (frac >=
+// 0.5).  u < 0 (whose reference result is 0 or negative), u >= 2^22 and NaN
+// return -1 or a value >= 2^22, both out of any image.
+__device__ __forceinline__ int round_px(float u)
+{
+  if (!(u >= 0.0f))
+    return -1;
+  if (u >= 4194304.0f)
+    return 1 << 22;
+  const float big = 8388608.0f; // 2^23
+  const float f = __fadd_rd(u, big);
+  const int fl = __float_as_int(f) - __float_as_int(big);
+  const float frac = __fsub_rn(u, __fsub_rn(f, big));
+  return fl + (frac >= 0.5f ? 1 : 0);
+}
 
 struct Cam
 {

@@ -196,8 +196,7 @@ class BatchDepthmap:
         return c.value
 
     KERNEL_KINDS = ("quadtree", "cost", "pyramid", "msg_init", "bp_sweep", "extract",
-                    "up_weights", "row_solve", "col_solve", "fuse_transform", "fuse_fill",
-                    "fuse_update")
+                    "row_solve", "col_solve", "fuse_transform", "fuse_fill", "fuse_update")
 
     def stream_ptr(self) -> int:
         """cudaStream_t the batch's kernels run on (for timing events)."""

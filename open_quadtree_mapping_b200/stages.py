@@ -37,7 +37,7 @@ def quadtree(img: torch.Tensor, params: Params = Params()) -> torch.Tensor:
     H, W = img.shape
     levels = torch.empty((H, W), dtype=torch.uint8, device=img.device)
     pc = _pc(params)
-    _lib.check(_lib.lib().qm_quadtree(_ptr(img), W, H, W, ctypes.byref(pc), _ptr(levels),
+    _lib.check(_lib.lib().qm_quadtree(_ptr(img), W, W, H, ctypes.byref(pc), _ptr(levels),
                                       _stream()))
     return levels
 
@@ -57,7 +57,7 @@ def cost_volume(ref: torch.Tensor, levels: torch.Tensor, slots, T_slot_ref, cam,
     cost = torch.empty((H // 4, W // 4, params.num_hyp), dtype=torch.float32, device=ref.device)
     c = _lib.QmCamera(*[float(v) for v in cam])
     pc = _pc(params)
-    _lib.check(_lib.lib().qm_cost_volume(_ptr(ref), W, H, W, ctypes.byref(c), _ptr(levels), F,
+    _lib.check(_lib.lib().qm_cost_volume(_ptr(ref), W, W, H, ctypes.byref(c), _ptr(levels), F,
                                          ptrs, W, T.ctypes.data, ctypes.byref(pc), _ptr(cost),
                                          _stream()))
     return cost

@@ -187,8 +187,9 @@ void quadtree_levels(const uint8_t *img, int w, int h, int max_level, int min_le
 // [2, W-2) x [2, H-2), scored by the SAD of the 3x3 reference patch against
 // the 3x3 measurement patch whose offsets are rotated by the top-left 2x2 of
 // R_f (depth_extract.cu:183-199).  The cost is sum/n_valid/255, or 100 when
-// no slot is valid.  Every term of the SAD is an integer, so the sum is exact
-// in any order.
+// no slot is valid, then divided by the number of hypotheses (the writer
+// count normalize_the_cost divides by).  Every term of the SAD is an integer,
+// so the sum is exact in any order.
 template <typename R>
 void cost_volume(const uint8_t *ref, int w, int h, const int *levels, int nslots,
                  const uint8_t *const *slot_img, const float *T, const Cam &cam,
@@ -262,7 +263,10 @@ void cost_volume(const uint8_t *ref, int w, int h, const int *levels, int nslots
           c = (R)sad / (R)nvalid / (R)255;
         else
           c = (R)100;
-        out[d] = c / (R)1; // normalize_the_cost: one writer per visited cell
+        // normalize_the_cost divides by the cell's writer count: every
+        // hypothesis thread of slot row 0 adds 1 (depth_extract.cu:219-228),
+        // so the count is the number of hypotheses.
+        out[d] = c / (R)D;
       }
     }
   });

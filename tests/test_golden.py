@@ -1,0 +1,77 @@
+"""The oracle pinned against the reference's own kernels.
+
+tests/golden/*.npz are dumps of the reference's CUDA kernels (built from its
+sources for sm_100a with -use_fast_math, run on a B200 by
+tests/golden/make_golden.py) on seeded synthetic inputs.  The oracle uses
+IEEE arithmetic where the reference build uses fast-math divisions and
+rsqrtf, so: levels, node masks and fusion tables are bit-exact; costs agree
+to the last bits except where a rounded projection falls within a fast-math
+error of a .5 boundary (a handful of cells); labels agree except at those.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from open_quadtree_mapping_b200.params import Params
+
+EXTRACT = ["ref_extract_64x48", "ref_extract_160x128", "ref_extract_320x240"]
+
+
+def _load(name):
+    path = os.path.join(GOLDEN, name + ".npz")
+    if not os.path.exists(path):
+        pytest.fail("missing golden fixture %s" % path)
+    return np.load(path)
+
+
+@pytest.mark.parametrize("name", EXTRACT)
+def test_oracle_extract_vs_reference_kernels(name, oracle_mod):
+    z = _load(name)
+    ref = z["ref"]
+    slots = [z["ring"][k] for k in z["slots"]]
+    T = z["T_ring_ref"][z["slots"]]
+    cam = tuple(float(c) for c in z["cam"])
+    o = oracle_mod.extract_depth(ref, slots, T, cam, Params(), want_messages=True)
+    assert np.array_equal(o["levels"], z["levels"])
+    if "cost" in z.files:
+        rc = z["cost"]
+        close = np.isclose(o["cost"], rc, rtol=1e-6, atol=1e-9)
+        assert close.mean() > 0.999, close.mean()  # elements off by a straddle
+        assert np.abs(o["cost"] - rc).max() < 1e-2
+    lab = z["labels"]
+    node = lab >= 0
+    assert np.array_equal(o["labels"] >= 0, node)
+    agree = (o["labels"][node] == lab[node]).mean()
+    assert agree > 0.999, agree
+    sp = z["sparse"]
+    m = sp != 0
+    assert np.array_equal(o["sparse"] != 0, m)
+    rel = np.abs(o["sparse"][m] - sp[m]) / sp[m]
+    # a straddle-affected cost moves the parabola of its cell
+    assert np.mean(rel < 1e-6) > 0.99
+    d = z["dense"]
+    fin = np.isfinite(d)
+    assert np.array_equal(np.isfinite(o["dense"]), fin)
+    reld = np.abs(o["dense"][fin] - d[fin]) / np.abs(d[fin])
+    assert np.percentile(reld, 99) < 1e-4
+    assert np.median(reld) < 1e-6
+    if "messages" in z.files:
+        assert np.allclose(o["messages"], z["messages"], rtol=0, atol=1e-6)
+
+
+def test_oracle_fuse_vs_reference_kernels(oracle_mod):
+    z = _load("ref_fuse_160x128")
+    cam = tuple(float(c) for c in z["cam"])
+    dense = z["dense"].astype(np.float32)
+    d1, s1, t1, c1 = oracle_mod.fuse(dense, np.zeros((128, 160, 4), np.float32), z["T1"], cam)
+    assert np.array_equal(d1, z["fused1"])
+    assert np.array_equal(t1, z["table1"])
+    assert np.allclose(s1, z["seeds1"], rtol=2e-5, atol=1e-7)
+    d2, s2, t2, c2 = oracle_mod.fuse(dense, z["seeds1"], z["T2"], cam)
+    ok = c2 == 0
+    assert ok.mean() > 0.9
+    assert np.array_equal(t2[ok], z["table2"][ok])
+    assert np.array_equal(d2[ok], z["fused2"][ok])
+    assert np.allclose(s2[ok], z["seeds2"][ok], rtol=2e-5, atol=1e-7)

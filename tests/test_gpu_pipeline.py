@@ -24,14 +24,17 @@ def test_facade_matches_oracle_replay(oracle_mod, gpu):
     policy, the debug map (sparse BP depths) is bit-exact with the oracle in
     IEEE mode, and the fused depth agrees with an oracle replay."""
     from open_quadtree_mapping_b200.depthmap import Depthmap
-    imgs, Ts, gts = sequence(1, 16, W, H)
+    n_frames = 40
+    imgs, Ts, gts = sequence(1, n_frames, W, H)
     p = Params(arith=ARITH_IEEE)  # the reference's hypothesis range
     dm = Depthmap(W, H, F_PX, W / 2.0, F_PX, H / 2.0, semi2dense_ratio=1, params=p)
     pol = PolicyReplay(num_slots=5)
     cam = (F_PX, F_PX, W / 2.0, H / 2.0)
     seeds = np.zeros((H, W, 4), np.float32)
     n_dense = 0
-    for i in range(16):
+    n_valid = 0
+    n_oracle_valid = 0
+    for i in range(n_frames):
         has = dm.add_frames(imgs[i], Ts[i])
         r = pol.add(i, Ts[i])
         assert has == (r["outcome"] in ("first", "dense")), (i, r["outcome"])
@@ -50,15 +53,20 @@ def test_facade_matches_oracle_replay(oracle_mod, gpu):
         seeds = new_seeds.astype(np.float32)
         depth = dm.getDepthmap()
         valid = fused > 0
+        n_oracle_valid += valid.sum()
         assert (depth > 0).mean() == pytest.approx(valid.mean(), abs=2e-3)
         both = valid & (depth > 0)
-        rel = np.abs(depth[both] - fused[both]) / fused[both]
-        assert np.percentile(rel, 99) < 1e-5, np.percentile(rel, 99)
+        n_valid += both.sum()
+        if both.any():
+            rel = np.abs(depth[both] - fused[both]) / fused[both]
+            assert np.percentile(rel, 99) < 1e-5, np.percentile(rel, 99)
         assert np.array_equal(dm.getReferenceImage(), imgs[i])
         T_wr = dm.getT_world_ref()
         from oracle.policy import se3_inv
         assert np.array_equal(T_wr.reshape(12), se3_inv(Ts[i]))
-    assert n_dense >= 3
+    assert n_dense >= 20
+    # the fused output turns valid only after ~15 consistent updates
+    assert n_valid == pytest.approx(n_oracle_valid, rel=0.01, abs=50)
 
 
 def test_batch_equals_plain_and_graph_equals_eager(gpu):

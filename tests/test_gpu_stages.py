@@ -69,8 +69,10 @@ def test_reference_mode_agrees_with_oracle(W, H, D, F, stream, oracle_mod, gpu):
     g = _gpu_extract(kf, p, gpu)
     o = oracle_mod.extract_depth(kf.ref, kf.meas, kf.T_meas_ref, cam_of(kf), p)
     assert np.array_equal(g["levels"], o["levels"])
-    cost_diff = (g["cost"] != o["cost"]).any(axis=2).mean()
-    assert cost_diff < 0.05, cost_diff
+    # fast-math divisions differ from IEEE in the last bits; a rounded
+    # projection near a .5 boundary changes one SAD term
+    close = np.isclose(g["cost"], o["cost"], rtol=1e-6, atol=1e-9).mean()
+    assert close > 0.999, close
     node = o["labels"] >= 0
     assert np.array_equal(g["labels"] >= 0, node)
     agree = (g["labels"][node] == o["labels"][node]).mean()
@@ -115,8 +117,11 @@ def test_textureless_image(oracle_mod, gpu):
 
 
 def test_fuse_vs_oracle(oracle_mod, gpu):
-    """Two fusion steps on a real keyframe pair: table bit-exact (IEEE
-    transform), fused depth and seeds within FP64 tolerance."""
+    """Twenty fusion steps on a real keyframe (nineteen static, then a small
+    motion): table bit-exact (IEEE transform), fused depth and seeds within
+    FP64 tolerance of the oracle's FP64 update on the same float seeds.  The
+    first outputs are all -1: the prior inlier ratio starts at 0.5 and only
+    passes 0.6 after ~15 consistent updates (depth_fusion.cu:175-210)."""
     from open_quadtree_mapping_b200 import stages
     kf = keyframe(3, 160, 128, 3)
     p = Params.for_range(64, 0.5, 50.0, arith=ARITH_IEEE)
@@ -124,25 +129,25 @@ def test_fuse_vs_oracle(oracle_mod, gpu):
     o = oracle_mod.extract_depth(kf.ref, kf.meas, kf.T_meas_ref, cam, p)
     dense = o["dense"].astype(np.float32)
     seeds = np.zeros((128, 160, 4), np.float32)
-    T = np.eye(3, 4, dtype=np.float32).reshape(12)
-    gd, gs_in, gs_out, gt = stages.fuse(torch.from_numpy(dense).to(gpu),
-                                        torch.from_numpy(seeds).to(gpu), T, cam, p)
-    od, os_, ot, oc = oracle_mod.fuse(dense.astype(np.float64), seeds, T, cam)
-    assert np.array_equal(gt.cpu().numpy(), ot)
-    assert np.allclose(gd.cpu().numpy(), od, rtol=FUSE_RTOL_F64)
-    seeds2 = gs_out.cpu().numpy()
-    assert np.allclose(seeds2, os_, rtol=FUSE_RTOL_F64, atol=1e-9)
-    # second step: a small motion, seeds now carry information
-    T2 = np.eye(3, 4, dtype=np.float32)
-    T2[0, 3] = 0.02
-    gd2, _, gs2, gt2 = stages.fuse(torch.from_numpy(dense).to(gpu),
-                                   torch.from_numpy(seeds2).to(gpu), T2.reshape(12), cam, p)
-    od2, os2, ot2, oc2 = oracle_mod.fuse(dense.astype(np.float64), seeds2, T2.reshape(12), cam)
-    assert np.array_equal(gt2.cpu().numpy(), ot2)
-    good = od2 > 0
-    assert good.mean() > 0.3
-    assert np.allclose(gd2.cpu().numpy(), od2, rtol=FUSE_RTOL_F64)
-    assert np.allclose(gs2.cpu().numpy(), os2, rtol=FUSE_RTOL_F64, atol=1e-9)
+    valid = []
+    for step in range(20):
+        T = np.eye(3, 4, dtype=np.float32)
+        if step == 19:
+            T[0, 3] = 0.02
+        T = T.reshape(12)
+        gd, _, gs, gt = stages.fuse(torch.from_numpy(dense).to(gpu),
+                                    torch.from_numpy(seeds).to(gpu), T, cam, p)
+        od, os_, ot, _ = oracle_mod.fuse(dense.astype(np.float64), seeds, T, cam)
+        assert np.array_equal(gt.cpu().numpy(), ot), step
+        gd = gd.cpu().numpy()
+        assert np.array_equal(gd > 0, od > 0), step
+        assert np.allclose(gd, od, rtol=FUSE_RTOL_F64), step
+        gs = gs.cpu().numpy()
+        assert np.allclose(gs, os_, rtol=FUSE_RTOL_F64, atol=1e-9), step
+        valid.append((gd > 0).mean())
+        seeds = gs
+    assert valid[0] == 0.0
+    assert max(valid) > 0.3, valid
 
 
 def test_invalid_arguments_are_rejected(gpu):

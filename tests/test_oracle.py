@@ -54,14 +54,15 @@ def test_cost_identity_pose_is_zero(oracle_mod):
     assert (cost[0] == 0).all() and (cost[:, 0] == 0).all()
 
 
-def test_cost_out_of_view_is_100(oracle_mod):
+def test_cost_out_of_view_is_100_over_d(oracle_mod):
     kf = keyframe(0, 160, 128)
     p = Params.for_range(64, 0.5, 50.0)
     lv = oracle_mod.quadtree(kf.ref, p)
     T = np.eye(3, 4, dtype=np.float32)
     T[0, 3] = 1e4  # moved far sideways: nothing projects into the image
     cost, valid = oracle_mod.cost_volume(kf.ref, lv, [kf.ref], T.reshape(1, 12), cam_of(kf), p)
-    assert (cost[valid == 1] == 100).all()
+    # 100 for no valid slot, divided by the writer count (the hypothesis count)
+    assert (cost[valid == 1] == np.float32(100) / np.float32(64)).all()
 
 
 def _tree_sum(v):
