@@ -63,7 +63,7 @@ def test_invalid_arguments_without_gpu(L):
     assert L.qm_bp_workspace_size(64, 64, ctypes.byref(p), ctypes.byref(n)) == _lib.QM_OK
     assert n.value > 0
     assert L.qm_upsample_workspace_size(752, 480, ctypes.byref(n)) == _lib.QM_OK
-    assert n.value >= 752 * 480 * 32
+    assert n.value >= 752 * 480 * 8  # the row-pass result, float2 per pixel
     h = ctypes.c_void_p()
     assert L.qm_depthmap_create(None, 64, 64, 1, 1, 1, 1, 1, None, 0) == _lib.QM_ERR_INVALID_ARG
     assert L.qm_depthmap_create(ctypes.byref(h), 64, 64, 50, 32, 50, 32, 0, None, 0) != _lib.QM_OK
