@@ -163,8 +163,8 @@ def algorithmic_bytes(levels_list, params):
     P = W * H
     C = (W // 4) * (H // 4)
     by = {k: 0.0 for k in ("quadtree", "cost", "pyramid", "msg_init", "bp_sweep", "extract",
-                           "up_weights", "row_solve", "col_solve", "fuse_transform",
-                           "fuse_fill", "fuse_update")}
+                           "row_solve", "col_solve", "fuse_transform", "fuse_fill",
+                           "fuse_update")}
     for lv in levels_list:
         cells = bp_updated_cells(lv, params)
         by["quadtree"] += 2 * P
@@ -180,9 +180,9 @@ def algorithmic_bytes(levels_list, params):
             n = sum(counts[i & 1] for i in range(it))
             by["bp_sweep"] += 36 * D * n
         by["extract"] += C * (20 * D + 4)
-        by["up_weights"] += P * (1 + 8)
-        by["row_solve"] += P * (4 + 4 + 24 + 24 + 8)
-        by["col_solve"] += P * (4 + 8 + 24 + 24 + 4)
+        # both solves derive the smoothness weights from the image in-kernel
+        by["row_solve"] += P * (4 + 1 + 8)
+        by["col_solve"] += P * (8 + 1 + 4)
         by["fuse_transform"] += P * 32
         by["fuse_fill"] += P * 12
         by["fuse_update"] += P * 52

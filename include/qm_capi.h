@@ -193,7 +193,8 @@ int qm_cost_volume(const uint8_t *ref, size_t ref_pitch, int width, int height,
  * seed_matrix.cu:530).  labels: device int32 (height/4)*(width/4) winning
  * hypothesis per cell, -1 where the cell is not a node origin (NULL to
  * skip).  messages: device f32 4*(height/4)*(width/4)*num_hyp final level-0
- * messages in the order up, down, left, right (NULL to skip). */
+ * messages in the order up, down, left, right (NULL to skip).  cost,
+ * messages and workspace must be 16-byte aligned (cudaMalloc'd memory is). */
 int qm_bp_workspace_size(int width, int height, const qm_params *p, size_t *bytes);
 int qm_bp_extract(const float *cost, int width, int height, const uint8_t *levels,
                   const qm_params *p, float *sparse, int32_t *labels, float *messages,

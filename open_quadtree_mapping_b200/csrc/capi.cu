@@ -459,6 +459,9 @@ int qm_bp_extract(const float *cost, int width, int height, const uint8_t *level
     const size_t need = bp_workspace(width, height, q);
     if (workspace_bytes < need || !workspace)
       throw CudaError{QM_ERR_WORKSPACE, "BP workspace too small"};
+    // the pyramid and message kernels move float4 groups
+    require(((uintptr_t)cost | (uintptr_t)messages | (uintptr_t)workspace) % 16 == 0,
+            "cost, messages and workspace must be 16-byte aligned");
     qm::JobDesc J = base_desc(width, height, q);
     J.levels = const_cast<uint8_t *>(levels);
     J.sparse = sparse;

@@ -4,7 +4,7 @@
 // fuse_output_depth (seed_matrix.cu:448-597):
 //   quadtree -> cost -> pyramid(1..L-1) -> zero messages(L-1) ->
 //   for level L-1..0: [message upsample] + bp half-sweeps ->
-//   extraction -> weights -> row solve -> column solve ->
+//   extraction -> row solve -> column solve ->
 //   fuse transform -> hole fill -> fuse update.
 // Every stage is one launch over all active jobs (one per hypothesis count
 // for the warp-per-cell BP kernels).  The reference runs 60-70 launches per
@@ -15,6 +15,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <cmath>
 #include <set>
 
 namespace qm
@@ -56,11 +57,12 @@ std::vector<int> stage_blocks(const Shape &s, const JobLayout &lay, const qm_par
   const int D = s.D;
   b[st.qt()] = cdiv(s.W, T) * cdiv(s.H, T);
   b[st.cost()] = cdiv((long)lay.lw[0] * lay.lh[0] * D, kFlatThreads);
+  // pyramid and message kernels move float4 groups of hypotheses
   for (int l = 1; l < L; ++l)
-    b[st.pyr(l)] = cdiv((long)lay.lw[l] * lay.lh[l] * D, kFlatThreads);
-  b[st.mzero()] = cdiv((long)lay.lw[L - 1] * lay.lh[L - 1] * D, kFlatThreads);
+    b[st.pyr(l)] = cdiv((long)lay.lw[l] * lay.lh[l] * (D / 4), kFlatThreads);
+  b[st.mzero()] = cdiv((long)lay.lw[L - 1] * lay.lh[L - 1] * (D / 4), kFlatThreads);
   for (int l = 0; l + 1 < L; ++l)
-    b[st.mup(l)] = cdiv((long)lay.lw[l] * lay.lh[l] * D, kFlatThreads);
+    b[st.mup(l)] = cdiv((long)lay.lw[l] * lay.lh[l] * (D / 4), kFlatThreads);
   for (int l = 0; l < L; ++l)
     b[st.sweep(l)] = cdiv((long)((lay.lw[l] + 1) / 2) * lay.lh[l], kCellWarps);
   b[st.extract()] = cdiv((long)lay.lw[0] * lay.lh[0], kCellWarps);
@@ -173,12 +175,23 @@ KParams kparams(const qm_params &p)
   return k;
 }
 
+bool rigid_enough(const float *T)
+{
+  for (int k = 0; k < 12; ++k)
+    if (!std::isfinite(T[k]))
+      return false;
+  return std::fabs(T[0]) + std::fabs(T[1]) <= 1.5f && std::fabs(T[4]) + std::fabs(T[5]) <= 1.5f;
+}
+
 int dedupe_slots(int F, const uint8_t *const *ptrs, const float *T, const uint8_t **out_ptrs,
                  float *out_T, int *out_w)
 {
   int n = 0;
   for (int f = 0; f < F; ++f)
   {
+    if (!rigid_enough(T + 12 * f))
+      throw CudaError{QM_ERR_INVALID_ARG,
+                      "measurement pose is not a rigid transform (finite, rotation rows bounded)"};
     int k = 0;
     while (k < n && !(out_ptrs[k] == ptrs[f] &&
                       std::memcmp(out_T + 12 * k, T + 12 * f, 12 * sizeof(float)) == 0))

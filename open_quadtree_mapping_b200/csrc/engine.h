@@ -96,9 +96,15 @@ std::string validate(const Shape &s, const qm_params &p);
 
 KParams kparams(const qm_params &p);
 
+// True when the 3x4 pose is finite and its rotation rows satisfy
+// |r00| + |r01| <= 1.5 and |r10| + |r11| <= 1.5 (every rotation does): the
+// cost kernel's rotated 3x3 patch then stays inside the measurement image.
+bool rigid_enough(const float *T);
+
 // Merges measurement slots with the same image and pose: writes the unique
 // slots (first-occurrence order) with their multiplicities and returns how
-// many there are.
+// many there are.  Throws CudaError(QM_ERR_INVALID_ARG) for a pose that is
+// not rigid_enough.
 int dedupe_slots(int F, const uint8_t *const *ptrs, const float *T, const uint8_t **out_ptrs,
                  float *out_T, int *out_w);
 

@@ -44,8 +44,11 @@ struct HypLayout
   static constexpr int P = pow2_ceil(D);   // tree width
 };
 
-// Stride-halving tree sum over D values held as v[k] = value(lane + 32k);
-// the result is valid in lane 0.
+// Stride-halving tree sum over D values held as v[k] = value(lane + 32k).
+// Strides >= 32 combine register slots; strides 16..1 run as an xor
+// butterfly.  Lane 0 performs exactly the reference's additions, and since
+// a + b == b + a bit for bit, every lane ends with lane 0's value, so no
+// broadcast is needed.
 template <int D>
 __device__ __forceinline__ float tree_sum(float (&v)[HypLayout<D>::NV])
 {
@@ -67,8 +70,22 @@ __device__ __forceinline__ float tree_sum(float (&v)[HypLayout<D>::NV])
   float r = a[0];
 #pragma unroll
   for (int o = (P / 2 < 16 ? P / 2 : 16); o > 0; o >>= 1)
-    r += __shfl_down_sync(0xffffffffu, r, o);
+    r += __shfl_xor_sync(0xffffffffu, r, o);
   return r;
+}
+
+// Order-preserving map between floats and signed ints (an involution), so a
+// float minimum can use the integer warp reduction.
+__device__ __forceinline__ int order_key(float f)
+{
+  const int b = __float_as_int(f);
+  return b ^ ((b >> 31) & 0x7fffffff);
+}
+
+__device__ __forceinline__ float warp_min_redux(float v)
+{
+  const int k = __reduce_min_sync(0xffffffffu, order_key(v));
+  return __int_as_float(k ^ ((k >> 31) & 0x7fffffff));
 }
 
 template <int D>
@@ -124,6 +141,10 @@ __device__ __forceinline__ float mean_of(float sum)
   return sum / (float)D;
 }
 
+// The three kernels below move whole float4 groups of hypotheses (D is a
+// multiple of 16 for every supported count, and every cell row starts on a
+// 16-byte boundary); each component keeps its own arithmetic.
+
 // ------------------------------------------------------------- pyramid
 // cost_distribute (bpextract.cu:169-198): L_l(x,y) = sum of the existing 2x2
 // children, x offset outer, y offset inner, starting from 0.
@@ -134,21 +155,28 @@ __global__ void __launch_bounds__(kFlatThreads)
   const JobDesc &J = job_of(B, lb);
   const LevelDesc &Lf = J.lv[level - 1];
   const LevelDesc &Lc = J.lv[level];
-  const int D = J.D;
+  const int D4 = J.D / 4;
   const long t = (long)lb * blockDim.x + threadIdx.x;
-  if (t >= (long)Lc.w * Lc.h * D)
+  if (t >= (long)Lc.w * Lc.h * D4)
     return;
-  const int cell = (int)(t / D);
-  const int d = (int)(t - (long)cell * D);
+  const int cell = (int)(t / D4);
+  const int q = (int)(t - (long)cell * D4);
   const int x = cell % Lc.w, y = cell / Lc.w;
-  float s = 0.0f;
+  const float4 *src = reinterpret_cast<const float4 *>(Lf.data);
+  float4 s = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 #pragma unroll
   for (int i = 0; i < 2; ++i)
 #pragma unroll
     for (int jj = 0; jj < 2; ++jj)
       if (2 * x + i < Lf.w && 2 * y + jj < Lf.h)
-        s += Lf.data[((size_t)(2 * y + jj) * Lf.w + (2 * x + i)) * D + d];
-  Lc.data[(size_t)cell * D + d] = s;
+      {
+        const float4 v = src[((size_t)(2 * y + jj) * Lf.w + (2 * x + i)) * D4 + q];
+        s.x += v.x;
+        s.y += v.y;
+        s.z += v.z;
+        s.w += v.w;
+      }
+  reinterpret_cast<float4 *>(Lc.data)[(size_t)cell * D4 + q] = s;
 }
 
 // Messages of the coarsest level start at zero (bpextract.cu:87-90).
@@ -158,13 +186,13 @@ __global__ void __launch_bounds__(kFlatThreads)
   int lb;
   const JobDesc &J = job_of(B, lb);
   const LevelDesc &L = J.lv[level];
-  const long n = (long)L.w * L.h * J.D;
+  const long n = (long)L.w * L.h * (J.D / 4);
   const long t = (long)lb * blockDim.x + threadIdx.x;
   if (t >= n)
     return;
 #pragma unroll
   for (int m = 0; m < 4; ++m)
-    L.msg[m][t] = 0.0f;
+    reinterpret_cast<float4 *>(L.msg[m])[t] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
 
 // upsample (bpextract.cu:374-395): every cell of level l starts from the
@@ -176,17 +204,17 @@ __global__ void __launch_bounds__(kFlatThreads)
   const JobDesc &J = job_of(B, lb);
   const LevelDesc &F = J.lv[level];
   const LevelDesc &C = J.lv[level + 1];
-  const int D = J.D;
+  const int D4 = J.D / 4;
   const long t = (long)lb * blockDim.x + threadIdx.x;
-  if (t >= (long)F.w * F.h * D)
+  if (t >= (long)F.w * F.h * D4)
     return;
-  const int cell = (int)(t / D);
-  const int d = (int)(t - (long)cell * D);
+  const int cell = (int)(t / D4);
+  const int q = (int)(t - (long)cell * D4);
   const int x = cell % F.w, y = cell / F.w;
-  const size_t src = ((size_t)(y >> 1) * C.w + (x >> 1)) * D + d;
+  const size_t src = ((size_t)(y >> 1) * C.w + (x >> 1)) * D4 + q;
 #pragma unroll
   for (int m = 0; m < 4; ++m)
-    F.msg[m][t] = C.msg[m][src];
+    reinterpret_cast<float4 *>(F.msg[m])[t] = reinterpret_cast<const float4 *>(C.msg[m])[src];
 }
 
 // ------------------------------------------------------------- sweep
@@ -256,26 +284,19 @@ __global__ void __launch_bounds__(kCellWarps * 32)
       hv[k] = in ? v : FLT_MAX;
       lmin = fminf(lmin, hv[k]);
     }
-    const float hmin = warp_min(lmin);
+    const float hmin = warp_min_redux(lmin);
     float m[NV];
 #pragma unroll
     for (int k = 0; k < NV; ++k)
     {
       const int d = lane + 32 * k;
-      float prev = __shfl_up_sync(0xffffffffu, hv[k], 1);
-      float next = __shfl_down_sync(0xffffffffu, hv[k], 1);
-      if (k > 0)
-      {
-        const float wrap = __shfl_sync(0xffffffffu, hv[k > 0 ? k - 1 : 0], 31);
-        if (lane == 0)
-          prev = wrap;
-      }
-      if (k + 1 < NV)
-      {
-        const float wrap = __shfl_sync(0xffffffffu, hv[k + 1 < NV ? k + 1 : k], 0);
-        if (lane == 31)
-          next = wrap;
-      }
+      // h(d-1): lane-1's slot k, or for lane 0 lane 31's slot k-1; h(d+1):
+      // lane+1's slot k, or for lane 31 lane 0's slot k+1.  One shuffle each,
+      // the source lane choosing which register it offers.
+      const float up_src = (lane == 31 && k > 0) ? hv[k > 0 ? k - 1 : 0] : hv[k];
+      const float dn_src = (lane == 0 && k + 1 < NV) ? hv[k + 1 < NV ? k + 1 : k] : hv[k];
+      const float prev = __shfl_sync(0xffffffffu, up_src, (lane + 31) & 31);
+      const float next = __shfl_sync(0xffffffffu, dn_src, (lane + 1) & 31);
       float mv = hv[k];
       if (d > 0)
         mv = fminf(mv, prev + P1);
@@ -284,7 +305,7 @@ __global__ void __launch_bounds__(kCellWarps * 32)
       mv = fminf(mv, hmin + P2);
       m[k] = d < D ? mv : 0.0f;
     }
-    const float sum = __shfl_sync(0xffffffffu, tree_sum<D>(m), 0);
+    const float sum = tree_sum<D>(m);
     const float mean = mean_of<D, ARITH>(sum);
     float *out = L.msg[dir] + c * D;
 #pragma unroll

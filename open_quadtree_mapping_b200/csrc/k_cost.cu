@@ -27,13 +27,38 @@ namespace qm
 namespace
 {
 
+// floor(u + 0.5) for 0 <= u + 0.5 < 2^23 with two round-down additions: the
+// largest float <= u + 0.5 has the same floor as u + 0.5 (integers are
+// floats), and adding 2^23 rounded down leaves exactly 2^23 + floor in the
+// float, whose bit pattern minus that of 2^23 is the integer.  This equals the
+// reference's (int)((double)u + 0.5) on that range.
+__device__ __forceinline__ int round_half_up(float u)
+{
+  const float f = __fadd_rd(__fadd_rd(u, 0.5f), 8388608.0f);
+  return __float_as_int(f) - 0x4B000000;
+}
+
 template <class A>
 __global__ void __launch_bounds__(kFlatThreads)
     k_cost(const __grid_constant__ Batch B)
 {
+  __shared__ float4 s_pose[kMaxSlots * 3];
+  __shared__ const uint8_t *s_img[kMaxSlots];
+  __shared__ int s_w[kMaxSlots];
   int lb;
   const JobDesc &J = job_of(B, lb);
   const int D = J.D;
+  const int F = J.F;
+  // the job's (deduplicated) slots, staged once per block; every block
+  // belongs to one job
+  for (int i = threadIdx.x; i < F * 12; i += blockDim.x)
+    reinterpret_cast<float *>(s_pose)[i] = slot_pose(B, J.slot_base + i / 12)[i % 12];
+  for (int i = threadIdx.x; i < F; i += blockDim.x)
+  {
+    s_img[i] = slot_image(B, J.slot_base + i);
+    s_w[i] = slot_weight(B, J.slot_base + i);
+  }
+  __syncthreads();
   const long t = (long)lb * blockDim.x + threadIdx.x;
   const int ncell = J.cw * J.ch;
   if (t >= (long)ncell * D)
@@ -63,40 +88,38 @@ __global__ void __launch_bounds__(kFlatThreads)
   const float depth = A::hyp_depth(J.step, J.min_inv, d);
   const float3 p = A::scale(dir, depth);
   const int pitch = J.slot_pitch;
+  // (int)(u + 0.5) in [2, W-2) exactly when u in [1.5, W-2.5) (both bounds
+  // are floats, the comparisons exact; NaN fails)
+  const float ulo = 1.5f, uhi = (float)W - 2.5f, vhi = (float)H - 2.5f;
   int sad = 0, nvalid = 0;
-  for (int f = 0; f < J.F; ++f)
+  for (int f = 0; f < F; ++f)
   {
-    // generic loads: in single-keyframe calls the poses live in the kernel
-    // parameter, not in global memory
-    const float *Tg = slot_pose(B, J.slot_base + f);
     float T[12];
-#pragma unroll
-    for (int k = 0; k < 12; ++k)
-      T[k] = Tg[k];
+    const float4 t0 = s_pose[3 * f], t1 = s_pose[3 * f + 1], t2 = s_pose[3 * f + 2];
+    T[0] = t0.x, T[1] = t0.y, T[2] = t0.z, T[3] = t0.w;
+    T[4] = t1.x, T[5] = t1.y, T[6] = t1.z, T[7] = t1.w;
+    T[8] = t2.x, T[9] = t2.y, T[10] = t2.z, T[11] = t2.w;
     const float3 q = A::apply(T, p);
     const float2 uv = A::project(q, cam);
-    // (int)(u + 0.5) in double in the reference; round_px is its exact
-    // single-precision equivalent for the ranges these tests accept
-    const int px = round_px(uv.x);
-    const int py = round_px(uv.y);
-    if (px >= 2 && px < W - 2 && py >= 2 && py < H - 2)
+    if (uv.x >= ulo && uv.x < uhi && uv.y >= ulo && uv.y < vhi)
     {
-      const uint8_t *m = slot_image(B, J.slot_base + f);
+      const uint8_t *m = s_img[f];
       const float u2u = T[0], u2v = T[4], v2u = T[1], v2v = T[5];
-      int s = 0;
+      // The slot poses are validated as rigid on the host (|r00|+|r01| and
+      // |r10|+|r11| <= 1.5), so every patch coordinate + 0.5 lies in
+      // [0.5, W-0.5) x [0.5, H-0.5): no clamp needed.
+      unsigned s = 0;
 #pragma unroll
       for (int jj = -1; jj <= 1; ++jj)
 #pragma unroll
         for (int ii = -1; ii <= 1; ++ii)
         {
-          // In range for any rotation (|r00| + |r01| <= sqrt(2)); the clamp
-          // only guards against non-rigid poses.
-          const int chx = min(max(round_px(A::patch_coord(uv.x, u2u, ii, v2u, jj)), 0), W - 1);
-          const int chy = min(max(round_px(A::patch_coord(uv.y, u2v, ii, v2v, jj)), 0), H - 1);
-          s += abs(patch[ii + 1][jj + 1] - (int)__ldg(m + (size_t)chy * pitch + chx));
+          const int chx = round_half_up(A::patch_coord(uv.x, u2u, ii, v2u, jj));
+          const int chy = round_half_up(A::patch_coord(uv.y, u2v, ii, v2v, jj));
+          s = __usad((unsigned)patch[ii + 1][jj + 1], (unsigned)__ldg(m + chy * pitch + chx), s);
         }
-      const int wgt = slot_weight(B, J.slot_base + f);
-      sad += wgt * s;
+      const int wgt = s_w[f];
+      sad += wgt * (int)s;
       nvalid += wgt;
     }
   }

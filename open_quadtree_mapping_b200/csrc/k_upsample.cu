@@ -96,15 +96,16 @@ __device__ __forceinline__ Mat2 mul(const Mat2 &L, const Mat2 &R)
               L.c * R.b + L.d * R.d};
 }
 
-// rescale by a power of two (exact) so the largest entry is in [0.5, 1)
+// rescale by a power of two (exact) so the largest entry is in [1, 2): the
+// scale is built from the exponent field of the largest magnitude
 __device__ __forceinline__ Mat2 renorm(const Mat2 &M)
 {
   const double mx = fmax(fmax(fabs(M.a), fabs(M.b)), fmax(fabs(M.c), fabs(M.d)));
-  if (!(mx > 0.0))
-    return M;
-  int e;
-  frexp(mx, &e);
-  return Mat2{ldexp(M.a, -e), ldexp(M.b, -e), ldexp(M.c, -e), ldexp(M.d, -e)};
+  const int e = (__double2hiint(mx) >> 20) & 0x7ff; // mx = 1.f * 2^(e - 1023)
+  if (e == 0 || e >= 2046)
+    return M; // zero, subnormal, huge, inf or nan: leave as is
+  const double s = __hiloint2double((2046 - e) << 20, 0); // 2^-(e - 1023)
+  return Mat2{M.a * s, M.b * s, M.c * s, M.d * s};
 }
 
 __device__ __forceinline__ Mat2 shfl_up(const Mat2 &M, int off)
@@ -126,7 +127,9 @@ __device__ void solve_line(const LineBuf &b, double lam)
   const int s = min(lane * b.m, b.n);
   const int e = min(s + b.m, b.n);
   const int base = lane * b.mp; // smem position of element s
-  // -------- pivots: segment Moebius product (apply element s first)
+  // -------- pivots: segment Moebius product (apply element s first).  The
+  // entries grow by at most 1 + 2*lambda per element, far inside the double
+  // range for segments of <= 128 elements, so no per-step rescaling.
   Mat2 P{1.0, 0.0, 0.0, 1.0};
   for (int k = s; k < e; ++k)
   {
@@ -134,8 +137,9 @@ __device__ void solve_line(const LineBuf &b, double lam)
     const double wl = b.w[p];
     const double wr = b.w[k + 1 < b.n ? b.pos(k + 1) : 32 * b.mp];
     const double a = -lam * wl, bb = 1.0 + lam * (wl + wr), c = -lam * wr;
-    P = renorm(Mat2{c * P.c, c * P.d, bb * P.c - a * P.a, bb * P.d - a * P.b});
+    P = Mat2{c * P.c, c * P.d, bb * P.c - a * P.a, bb * P.d - a * P.b};
   }
+  P = renorm(P);
   // inclusive scan (later segments on the left), then exclusive
 #pragma unroll
   for (int off = 1; off < 32; off <<= 1)
@@ -147,8 +151,14 @@ __device__ void solve_line(const LineBuf &b, double lam)
   Mat2 E = shfl_up(P, 1);
   if (lane == 0)
     E = Mat2{1.0, 0.0, 0.0, 1.0};
-  double cp = E.b / E.d; // incoming pivot c'_{s-1} (0 for lane 0)
-  // -------- pivots of the segment (FP64), forward RHS composition (FP32)
+  const double z0 = E.b / E.d; // incoming pivot c'_{s-1} (0 for lane 0)
+  // -------- pivots of the segment (FP64), forward RHS composition (FP32).
+  // With the running product Q of the segment's Moebius maps, c'_k =
+  // (Q.a z0 + Q.b) / D_k where D_k = Q.c z0 + Q.d, and den_k = D_k / D_{k-1},
+  // so 1/den_k = D_{k-1} / D_k and c'_k = c_k / den_k.  Only the 2x2 products
+  // form the serial chain; the one division per element does not feed back.
+  Mat2 Q{1.0, 0.0, 0.0, 1.0};
+  double Dprev = 1.0;
   Aff F{1.0f, 0.0f, 0.0f};
   for (int k = s; k < e; ++k)
   {
@@ -156,8 +166,11 @@ __device__ void solve_line(const LineBuf &b, double lam)
     const double wl = b.w[p];
     const double wr = b.w[k + 1 < b.n ? b.pos(k + 1) : 32 * b.mp];
     const double a = -lam * wl, bb = 1.0 + lam * (wl + wr), c = -lam * wr;
-    const double inv = 1.0 / (bb - a * cp);
-    cp = c * inv;
+    Q = Mat2{c * Q.c, c * Q.d, bb * Q.c - a * Q.a, bb * Q.d - a * Q.b};
+    const double Dk = Q.c * z0 + Q.d;
+    const double inv = Dprev / Dk; // 1 / den_k
+    Dprev = Dk;
+    const double cp = c * inv;
     b.cp[p] = (float)cp;
     const float invf = (float)inv;
     b.dd[p] = invf;

@@ -154,26 +154,6 @@ __device__ __forceinline__ int slot_weight(const Batch &B, int slot)
 // the reference performs it on `float + 0.5`).
 __device__ __forceinline__ int trunc_int(double v) { return (int)v; }
 
-// (int)((double)u + 0.5) -- the reference's pixel rounding -- with
-// single-precision operations only, for callers that only use results >= 0
-// (every result below 0 is reported as -1).  Exact: for 0 <= u < 2^22,
-// adding 2^23 with round-down gives 2^23 + floor(u) exactly, floor(u) and the
-// fraction u - floor(u) are exact, and trunc(u + 0.5) = floor(u) + (frac >=
-// 0.5).  u < 0 (whose reference result is 0 or negative), u >= 2^22 and NaN
-// return -1 or a value >= 2^22, both out of any image.
-__device__ __forceinline__ int round_px(float u)
-{
-  if (!(u >= 0.0f))
-    return -1;
-  if (u >= 4194304.0f)
-    return 1 << 22;
-  const float big = 8388608.0f; // 2^23
-  const float f = __fadd_rd(u, big);
-  const int fl = __float_as_int(f) - __float_as_int(big);
-  const float frac = __fsub_rn(u, __fsub_rn(f, big));
-  return fl + (frac >= 0.5f ? 1 : 0);
-}
-
 struct Cam
 {
   float fx, fy, cx, cy;
