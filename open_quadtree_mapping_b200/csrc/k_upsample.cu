@@ -36,6 +36,8 @@
 // pass 1 + 8 read, 4 written.
 #include "launch.h"
 
+#include <atomic>
+
 namespace qm
 {
 
@@ -333,9 +335,34 @@ void prepare_upsample_kernels()
   cudaFuncSetAttribute(k_col_solve<ArithIeee>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
 }
 
+namespace
+{
+// Lines longer than about 1000 elements need more than the default 48 KB of
+// dynamic shared memory; the opt-in is a per-device function attribute, so
+// the launchers set it once for every device they launch on (stage calls may
+// run without an engine having been created on that device).
+std::atomic<unsigned long long> g_prepared_devices{0};
+
+void prepare_once_for_current_device()
+{
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+  {
+    prepare_upsample_kernels();
+    return;
+  }
+  const unsigned long long bit = 1ull << dev;
+  if (g_prepared_devices.load(std::memory_order_acquire) & bit)
+    return;
+  prepare_upsample_kernels();
+  g_prepared_devices.fetch_or(bit, std::memory_order_acq_rel);
+}
+} // namespace
+
 void launch_row_solve(const Batch &B, int blocks, KParams kp, int arith, int max_w,
                       cudaStream_t s)
 {
+  prepare_once_for_current_device();
   const size_t sm = row_solve_smem(max_w);
   if (arith == QM_ARITH_IEEE)
     k_row_solve<ArithIeee><<<blocks, kRowWarps * 32, sm, s>>>(B, kp, max_w);
@@ -346,6 +373,7 @@ void launch_row_solve(const Batch &B, int blocks, KParams kp, int arith, int max
 void launch_col_solve(const Batch &B, int blocks, KParams kp, int arith, int max_h,
                       cudaStream_t s)
 {
+  prepare_once_for_current_device();
   const size_t sm = col_solve_smem(max_h);
   if (arith == QM_ARITH_IEEE)
     k_col_solve<ArithIeee><<<blocks, kColLines * 32, sm, s>>>(B, kp, max_h);

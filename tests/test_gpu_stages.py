@@ -150,6 +150,45 @@ def test_fuse_vs_oracle(oracle_mod, gpu):
     assert max(valid) > 0.3, valid
 
 
+_UPSAMPLE_CHILD = r"""
+import sys, numpy as np, torch
+from open_quadtree_mapping_b200 import stages
+from open_quadtree_mapping_b200.params import ARITH_IEEE, Params
+z = np.load(sys.argv[1])
+dev = torch.device("cuda:0")
+d = stages.upsample(torch.from_numpy(z["sparse"]).to(dev), torch.from_numpy(z["img"]).to(dev),
+                    Params(arith=ARITH_IEEE))
+np.save(sys.argv[2], d.cpu().numpy())
+"""
+
+
+def _sparse_case(W, H, seed):
+    rng = np.random.default_rng(seed)
+    yy, xx = np.mgrid[0:H, 0:W]
+    img = (128 + 60 * np.sin(xx / 37.0) * np.cos(yy / 23.0)
+           + rng.normal(0, 8, (H, W))).clip(0, 255).astype(np.uint8)
+    sparse = np.where(rng.random((H, W)) < 0.05, rng.uniform(0.5, 20.0, (H, W)), 0.0)
+    return img, sparse.astype(np.float32)
+
+
+def test_upsample_long_lines_in_fresh_process(oracle_mod, gpu, tmp_path):
+    """Lines of 1280 and 720 samples need more than 48 KB of dynamic shared
+    memory: the stage call must opt in by itself, in a process where no depth
+    engine was ever created."""
+    import subprocess
+    import sys
+    W, H = 1280, 720
+    img, sparse = _sparse_case(W, H, 5)
+    np.savez(tmp_path / "in.npz", img=img, sparse=sparse)
+    root = str(__import__("pathlib").Path(__file__).resolve().parents[1])
+    subprocess.run([sys.executable, "-c", _UPSAMPLE_CHILD, str(tmp_path / "in.npz"),
+                    str(tmp_path / "out.npy")], check=True, cwd=root, timeout=300)
+    g = np.load(tmp_path / "out.npy")
+    p = Params(arith=ARITH_IEEE)
+    d64 = oracle_mod.upsample(sparse.astype(np.float64), img, p)
+    assert np.allclose(g, d64, rtol=UPSAMPLE_RTOL_F64, atol=0)
+
+
 def test_invalid_arguments_are_rejected(gpu):
     import ctypes
     from open_quadtree_mapping_b200 import _lib
