@@ -209,6 +209,21 @@ int qm_upsample(const float *sparse, const uint8_t *img, size_t img_pitch, int w
                 const qm_params *p, float *dense, void *workspace, size_t workspace_bytes,
                 void *stream);
 
+/* qm_upsample without a workspace argument: no counterpart in the reference
+ * (whose global_upsample cudaMallocs its buffers on every call).  For hosts
+ * that cannot allocate device memory per call (a plugin host without a CUDA
+ * allocator, a real-time loop that must not cudaMalloc after start-up).  It
+ * allocates nothing: the row-pass scratch is a fixed device array of this
+ * library of QM_UPSAMPLE_NOALLOC_MAX_PIXELS pixels (8 bytes each); larger
+ * images return QM_ERR_INVALID_ARG.  The first call on a device sets up that
+ * device (make it before any stream capture).  All calls on a device share
+ * the scratch: calls that can overlap on the device race and give undefined
+ * output, so issue them in order (e.g. on one stream).  Same limits as
+ * qm_upsample otherwise. */
+#define QM_UPSAMPLE_NOALLOC_MAX_PIXELS (1u << 20)
+int qm_upsample_noalloc(const float *sparse, const uint8_t *img, size_t img_pitch, int width,
+                        int height, const qm_params *p, float *dense, void *stream);
+
 /* fuse_transform, hole_filling and fuse_currentmap (depth_fusion.cu:48-213;
  * launch seed_matrix.cu:553-597).  depth: device f32 width*height, in:
  * upsampled depth, out: fused depth (mu' or -1).  seeds_in / seeds_out:

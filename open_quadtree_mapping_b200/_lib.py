@@ -87,6 +87,7 @@ _SIGS = {
     "qm_bp_extract": (_I, [_P, _I, _I, _P, ctypes.POINTER(QmParamsC), _P, _P, _P, _P, _S, _P]),
     "qm_upsample_workspace_size": (_I, [_I, _I, ctypes.POINTER(_S)]),
     "qm_upsample": (_I, [_P, _P, _S, _I, _I, ctypes.POINTER(QmParamsC), _P, _P, _S, _P]),
+    "qm_upsample_noalloc": (_I, [_P, _P, _S, _I, _I, ctypes.POINTER(QmParamsC), _P, _P]),
     "qm_fuse_workspace_size": (_I, [_I, _I, ctypes.POINTER(_S)]),
     "qm_fuse": (_I, [_P, _P, _P, _P, ctypes.POINTER(QmCamera), _I, _I,
                      ctypes.POINTER(QmParamsC), _P, _P, _S, _P]),
