@@ -172,9 +172,11 @@ def algorithmic_bytes(levels_list, params):
         sizes = [(w * h) for (w, h, _) in cells]
         for l in range(1, params.bp_levels):
             by["pyramid"] += 4 * D * (sizes[l - 1] + sizes[l])
-        by["msg_init"] += 16 * D * sizes[-1]
-        for l in range(params.bp_levels - 1):
-            by["msg_init"] += 16 * D * (sizes[l + 1] + sizes[l])
+        # message inheritance writes the four messages of the cells the
+        # quadtree test skips (copied from the parent level, zeros at the top)
+        for l, (w, h, counts) in enumerate(cells):
+            skipped = w * h - counts[0] - counts[1]
+            by["msg_init"] += 16 * D * skipped * (2 if l + 1 < params.bp_levels else 1)
         for l, (w, h, counts) in enumerate(cells):
             it = params.bp_iters[l]
             n = sum(counts[i & 1] for i in range(it))

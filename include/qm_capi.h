@@ -146,6 +146,11 @@ int qm_batch_run_resident(qm_batch *b);
 int qm_batch_device_depth(qm_batch *b, int stream, const float **dev_ptr);
 /* 1 = replay captured CUDA graphs (default), 0 = launch stage by stage. */
 int qm_batch_set_graphs(qm_batch *b, int enable);
+/* L2 budget, in bytes, of a job range of the belief propagation: each BP
+ * level runs over consecutive streams whose level costs and messages fit in
+ * it, so the range's half-sweeps hit L2.  0 = every level over all streams
+ * at once (the default).  Results do not depend on it. */
+int qm_batch_set_group_bytes(qm_batch *b, size_t bytes);
 /* Kernels launched by the last dense-pipeline run. */
 int qm_batch_last_launches(qm_batch *b, int *count);
 /* The cudaStream_t (as void*) every kernel of this batch is launched on;

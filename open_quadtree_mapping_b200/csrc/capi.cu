@@ -363,6 +363,14 @@ int qm_batch_set_graphs(qm_batch *b, int enable)
   });
 }
 
+int qm_batch_set_group_bytes(qm_batch *b, size_t bytes)
+{
+  return guarded([&] {
+    require(b != nullptr, "NULL handle");
+    b->set->engine().set_group_bytes(bytes);
+  });
+}
+
 int qm_batch_last_launches(qm_batch *b, int *count)
 {
   return guarded([&] {

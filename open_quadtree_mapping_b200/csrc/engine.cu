@@ -2,15 +2,18 @@
 //
 // Stage order of one run, after SeedMatrix::extract_depth and
 // fuse_output_depth (seed_matrix.cu:448-597):
-//   quadtree -> cost -> pyramid(1..L-1) -> zero messages(L-1) ->
-//   for level L-1..0: [message upsample] + bp half-sweeps ->
-//   extraction -> row solve -> column solve ->
-//   fuse transform -> hole fill -> fuse update.
+//   quadtree -> cost -> pyramid(1..L-1) ->
+//   for level L-1..0: message inheritance + bp half-sweeps
+//     (+ extraction at level 0) ->
+//   row solve -> column solve -> fuse transform -> hole fill -> fuse update.
 // Every stage is one launch over all active jobs (one per hypothesis count
-// for the warp-per-cell BP kernels).  The reference runs 60-70 launches per
-// keyframe with a cudaDeviceSynchronize after most and ~25 device
-// allocations; here a keyframe batch is ~45 launches, no allocation, and the
-// whole sequence is captured once per active set and replayed as a graph.
+// for the warp-per-cell BP kernels); optionally the BP stages of a level run
+// over consecutive job ranges whose level working set fits a byte budget, so
+// the half-sweeps of a range re-read their costs and messages from L2.  The
+// reference runs 60-70 launches per keyframe with a cudaDeviceSynchronize
+// after most and ~25 device allocations; here a batch needs no allocation,
+// and the whole sequence is captured once per active set and replayed as a
+// graph.
 #include "engine.h"
 
 #include <algorithm>
@@ -36,8 +39,7 @@ struct Stages
   int qt() const { return 0; }
   int cost() const { return 1; }
   int pyr(int l) const { return 2 + (l - 1); } // l = 1..L-1
-  int mzero() const { return 1 + L; }
-  int mup(int l) const { return 2 + L + l; } // l = 0..L-2
+  int inherit(int l) const { return 1 + L + l; } // l = 0..L-1
   int sweep(int l) const { return 1 + 2 * L + l; }
   int extract() const { return 1 + 3 * L; }
   int row() const { return 2 + 3 * L; }
@@ -53,16 +55,14 @@ std::vector<int> stage_blocks(const Shape &s, const JobLayout &lay, const qm_par
   const Stages st{p.bp_levels};
   std::vector<int> b(st.count(), 0);
   const int L = p.bp_levels;
-  const int T = quadtree_tile(p.qt_max_level);
   const int D = s.D;
-  b[st.qt()] = cdiv(s.W, T) * cdiv(s.H, T);
+  b[st.qt()] = quadtree_blocks(s.W, s.H, p.qt_max_level);
   b[st.cost()] = cdiv((long)lay.lw[0] * lay.lh[0] * D, kFlatThreads);
   // pyramid and message kernels move float4 groups of hypotheses
   for (int l = 1; l < L; ++l)
     b[st.pyr(l)] = cdiv((long)lay.lw[l] * lay.lh[l] * (D / 4), kFlatThreads);
-  b[st.mzero()] = cdiv((long)lay.lw[L - 1] * lay.lh[L - 1] * (D / 4), kFlatThreads);
-  for (int l = 0; l + 1 < L; ++l)
-    b[st.mup(l)] = cdiv((long)lay.lw[l] * lay.lh[l] * (D / 4), kFlatThreads);
+  for (int l = 0; l < L; ++l)
+    b[st.inherit(l)] = cdiv((long)lay.lw[l] * lay.lh[l] * (D / 4), kFlatThreads);
   for (int l = 0; l < L; ++l)
     b[st.sweep(l)] = cdiv((long)((lay.lw[l] + 1) / 2) * lay.lh[l], kCellWarps);
   b[st.extract()] = cdiv((long)lay.lw[0] * lay.lh[0], kCellWarps);
@@ -72,12 +72,67 @@ std::vector<int> stage_blocks(const Shape &s, const JobLayout &lay, const qm_par
   return b;
 }
 
-// Launches stages [first, last] of the sequence; B.prefix is replaced by
-// prefix[stage] (may be null for a single inline job).  When `prof` is given,
-// every launch is bracketed by a pair of events recorded on `s`.  Returns the
+// Block layout of every stage over the jobs of one launch sequence.
+struct StageTable
+{
+  int n = 0;                       // jobs
+  std::vector<int> hprefix;        // host, stage s: [s*(n+1), (s+1)*(n+1))
+  std::vector<const int *> prefix; // device copy per stage (null: one inline job)
+  std::vector<int> uniform;        // per stage: blocks per job when all agree, else 0
+  std::vector<int> dvals;          // hypothesis counts present
+  std::vector<size_t> level_bytes; // per job and BP level: data + messages
+  int max_w = 0, max_h = 0;        // longest lines of the row / column solves
+
+  int begin(int stage, int j) const { return hprefix[(size_t)stage * (n + 1) + j]; }
+  int blocks(int stage) const { return begin(stage, n); }
+
+  void add_jobs(const std::vector<std::vector<int>> &per_job, const std::vector<int> &ds)
+  {
+    n = (int)per_job.size();
+    const int ns = n ? (int)per_job[0].size() : 0;
+    hprefix.assign((size_t)ns * (n + 1), 0);
+    uniform.assign(ns, 0);
+    for (int st = 0; st < ns; ++st)
+    {
+      bool same = true;
+      for (int j = 0; j < n; ++j)
+      {
+        hprefix[(size_t)st * (n + 1) + j + 1] = hprefix[(size_t)st * (n + 1) + j] + per_job[j][st];
+        same = same && per_job[j][st] == per_job[0][st];
+      }
+      uniform[st] = (same && n > 0) ? per_job[0][st] : 0;
+    }
+    std::set<int> u(ds.begin(), ds.end());
+    dvals.assign(u.begin(), u.end());
+  }
+};
+
+// Consecutive job ranges [g[i], g[i+1]) whose BP level-`level` working sets
+// stay within `budget` bytes (at least one job per range); budget 0 = one
+// range.  Running the sweeps of a level range by range keeps that range's
+// costs and messages resident in L2 across the half-sweeps.
+std::vector<int> job_groups(const StageTable &T, int level, int L, size_t budget)
+{
+  std::vector<int> g{0};
+  size_t acc = 0;
+  for (int j = 0; j < T.n; ++j)
+  {
+    const size_t b = T.level_bytes.empty() ? 0 : T.level_bytes[(size_t)j * L + level];
+    if (budget > 0 && j > g.back() && acc + b > budget)
+    {
+      g.push_back(j);
+      acc = 0;
+    }
+    acc += b;
+  }
+  g.push_back(T.n);
+  return g;
+}
+
+// Launches stages [first, last] of the sequence.  When `prof` is given, every
+// launch is bracketed by a pair of events recorded on `s`.  Returns the
 // number of kernel launches.
-int enqueue_range(Batch B, const std::vector<const int *> &prefix, const std::vector<int> &blocks,
-                  const qm_params &p, const std::vector<int> &dvals, int max_w, int max_h,
+int enqueue_range(const Batch &B, const StageTable &T, const qm_params &p, size_t group_bytes,
                   int first, int last, cudaStream_t s, LaunchProfile *prof = nullptr)
 {
   const Stages st{p.bp_levels};
@@ -85,10 +140,14 @@ int enqueue_range(Batch B, const std::vector<const int *> &prefix, const std::ve
   const KParams kp = kparams(p);
   const int ar = p.arith;
   int n = 0;
-  auto in = [&](int stage) { return stage >= first && stage <= last && blocks[stage] > 0; };
-  auto at = [&](int stage) {
+  auto in = [&](int stage) { return stage >= first && stage <= last && T.blocks(stage) > 0; };
+  // the batch of stage `stage` restricted to jobs [j0, j1), and its grid
+  auto at = [&](int stage, int j0, int j1, int &grid) {
     Batch b = B;
-    b.prefix = prefix.empty() ? nullptr : prefix[stage];
+    b.prefix = T.prefix.empty() ? nullptr : T.prefix[stage];
+    b.uniform = T.uniform[stage];
+    b.block0 = T.begin(stage, j0);
+    grid = T.begin(stage, j1) - b.block0;
     return b;
   };
   auto launch = [&](int kind, auto &&fn) {
@@ -107,42 +166,61 @@ int enqueue_range(Batch B, const std::vector<const int *> &prefix, const std::ve
     }
     ++n;
   };
-  if (in(st.qt()))
-    launch(kQuadtree, [&] { launch_quadtree(at(st.qt()), blocks[st.qt()], kp, s); });
-  if (in(st.cost()))
-    launch(kCost, [&] { launch_cost(at(st.cost()), blocks[st.cost()], ar, s); });
+  // one launch of `stage` over all jobs
+  auto all = [&](int kind, int stage, auto &&fn) {
+    if (!in(stage))
+      return;
+    int grid = 0;
+    const Batch b = at(stage, 0, T.n, grid);
+    if (grid > 0)
+      launch(kind, [&] { fn(b, grid); });
+  };
+  all(kQuadtree, st.qt(), [&](const Batch &b, int g) { launch_quadtree(b, g, kp, s); });
+  all(kCost, st.cost(), [&](const Batch &b, int g) { launch_cost(b, g, ar, s); });
   for (int l = 1; l < L; ++l)
-    if (in(st.pyr(l)))
-      launch(kPyramid, [&] { launch_pyramid(at(st.pyr(l)), blocks[st.pyr(l)], l, s); });
-  if (in(st.mzero()))
-    launch(kMsgInit, [&] { launch_msg_zero(at(st.mzero()), blocks[st.mzero()], L - 1, s); });
+    all(kPyramid, st.pyr(l), [&](const Batch &b, int g) { launch_pyramid(b, g, l, s); });
+  // BP, coarse to fine; each level runs job range by job range (message
+  // inheritance, half-sweeps, and at level 0 the extraction)
   for (int l = L - 1; l >= 0; --l)
   {
-    if (l + 1 < L && in(st.mup(l)))
-      launch(kMsgInit, [&] { launch_msg_upsample(at(st.mup(l)), blocks[st.mup(l)], l, s); });
-    if (in(st.sweep(l)))
-      for (int it = 0; it < p.bp_iters[l]; ++it)
-        for (int d : dvals)
-          launch(kSweep, [&] {
-            launch_bp_sweep(at(st.sweep(l)), blocks[st.sweep(l)], d, l, it & 1, kp, ar, s);
+    const std::vector<int> groups = job_groups(T, l, L, group_bytes);
+    for (size_t gi = 0; gi + 1 < groups.size(); ++gi)
+    {
+      const int j0 = groups[gi], j1 = groups[gi + 1];
+      int grid = 0;
+      if (in(st.inherit(l)))
+      {
+        const Batch b = at(st.inherit(l), j0, j1, grid);
+        if (grid > 0)
+          launch(kMsgInit, [&] {
+            launch_msg_inherit(b, grid, l, p.bp_iters[l], p.qt_max_level, s);
           });
+      }
+      if (in(st.sweep(l)))
+      {
+        const Batch b = at(st.sweep(l), j0, j1, grid);
+        if (grid > 0)
+          for (int it = 0; it < p.bp_iters[l]; ++it)
+            for (int d : T.dvals)
+              launch(kSweep, [&] { launch_bp_sweep(b, grid, d, l, it, kp, ar, s); });
+      }
+      if (l == 0 && in(st.extract()))
+      {
+        const Batch b = at(st.extract(), j0, j1, grid);
+        if (grid > 0)
+          for (int d : T.dvals)
+            launch(kExtract, [&] { launch_extract(b, grid, d, ar, s); });
+      }
+    }
   }
-  if (in(st.extract()))
-    for (int d : dvals)
-      launch(kExtract, [&] { launch_extract(at(st.extract()), blocks[st.extract()], d, ar, s); });
-  if (in(st.row()))
-    launch(kRowSolve,
-           [&] { launch_row_solve(at(st.row()), blocks[st.row()], kp, ar, max_w, s); });
-  if (in(st.col()))
-    launch(kColSolve,
-           [&] { launch_col_solve(at(st.col()), blocks[st.col()], kp, ar, max_h, s); });
-  if (in(st.ftrans()))
-    launch(kFuseTransform,
-           [&] { launch_fuse_transform(at(st.ftrans()), blocks[st.ftrans()], ar, s); });
-  if (in(st.ffill()))
-    launch(kFuseFill, [&] { launch_fuse_fill(at(st.ffill()), blocks[st.ffill()], s); });
-  if (in(st.fupd()))
-    launch(kFuseUpdate, [&] { launch_fuse_update(at(st.fupd()), blocks[st.fupd()], s); });
+  all(kRowSolve, st.row(),
+      [&](const Batch &b, int g) { launch_row_solve(b, g, kp, ar, T.max_w, s); });
+  all(kColSolve, st.col(),
+      [&](const Batch &b, int g) { launch_col_solve(b, g, kp, ar, T.max_h, s); });
+  all(kFuseTransform, st.ftrans(),
+      [&](const Batch &b, int g) { launch_fuse_transform(b, g, ar, s); });
+  all(kFuseFill, st.ffill(), [&](const Batch &b, int g) { launch_fuse_fill(b, g, s); });
+  all(kFuseUpdate, st.fupd(), [&](const Batch &b, int g) { launch_fuse_update(b, g, s); });
   check(cudaGetLastError(), "kernel launch");
   return n;
 }
@@ -327,10 +405,8 @@ struct Plan
 {
   std::vector<int> active;
   int *d_prefix = nullptr;
-  std::vector<const int *> prefix; // per stage, into d_prefix
-  std::vector<int> blocks;         // per stage, total
-  std::vector<int> dvals;
-  int max_w = 0, max_h = 0; // longest lines of the row / column solves
+  StageTable table;
+  size_t group_bytes = 0; // the job grouping the graph was captured with
   cudaGraphExec_t exec = nullptr;
   ~Plan()
   {
@@ -494,33 +570,41 @@ Plan &Engine::plan_for(const std::vector<int> &active)
 {
   auto it = plans_.find(active);
   if (it != plans_.end())
-    return *it->second;
+  {
+    Plan &pl = *it->second;
+    if (pl.exec && pl.group_bytes != group_bytes_)
+    {
+      cudaGraphExecDestroy(pl.exec);
+      pl.exec = nullptr;
+    }
+    return pl;
+  }
   auto pl = std::make_unique<Plan>();
   pl->active = active;
-  const Stages st{params_.bp_levels};
-  const int ns = st.count();
+  const int L = params_.bp_levels;
   const int n = (int)active.size();
-  std::vector<int> h(ns * (n + 1), 0);
-  pl->blocks.assign(ns, 0);
-  std::set<int> ds;
+  std::vector<std::vector<int>> per_job;
+  std::vector<int> ds;
+  StageTable &T = pl->table;
   for (int i = 0; i < n; ++i)
   {
     const int j = active[i];
-    ds.insert(shapes_[j].D);
-    pl->max_w = std::max(pl->max_w, shapes_[j].W);
-    pl->max_h = std::max(pl->max_h, shapes_[j].H);
-    const std::vector<int> b = stage_blocks(shapes_[j], layouts_[j], params_);
-    for (int s = 0; s < ns; ++s)
-      h[s * (n + 1) + i + 1] = h[s * (n + 1) + i] + b[s];
+    ds.push_back(shapes_[j].D);
+    T.max_w = std::max(T.max_w, shapes_[j].W);
+    T.max_h = std::max(T.max_h, shapes_[j].H);
+    per_job.push_back(stage_blocks(shapes_[j], layouts_[j], params_));
+    for (int l = 0; l < L; ++l)
+      T.level_bytes.push_back((size_t)5 * layouts_[j].lw[l] * layouts_[j].lh[l] * shapes_[j].D *
+                              sizeof(float));
   }
-  for (int s = 0; s < ns; ++s)
-    pl->blocks[s] = h[s * (n + 1) + n];
-  pl->dvals.assign(ds.begin(), ds.end());
-  check(cudaMalloc((void **)&pl->d_prefix, sizeof(int) * h.size()), "device allocation");
-  check(cudaMemcpy(pl->d_prefix, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice),
+  T.add_jobs(per_job, ds);
+  const int ns = (int)T.uniform.size();
+  check(cudaMalloc((void **)&pl->d_prefix, sizeof(int) * T.hprefix.size()), "device allocation");
+  check(cudaMemcpy(pl->d_prefix, T.hprefix.data(), sizeof(int) * T.hprefix.size(),
+                   cudaMemcpyHostToDevice),
         "plan upload");
-  for (int s = 0; s < ns; ++s)
-    pl->prefix.push_back(pl->d_prefix + s * (n + 1));
+  for (int st = 0; st < ns; ++st)
+    T.prefix.push_back(pl->d_prefix + (size_t)st * (n + 1));
   Plan &ref = *pl;
   plans_[active] = std::move(pl);
   return ref;
@@ -565,8 +649,8 @@ int Engine::enqueue(Plan &pl, cudaStream_t s)
 {
   const Batch B = upload((int)pl.active.size(), s);
   const Stages st{params_.bp_levels};
-  return enqueue_range(B, pl.prefix, pl.blocks, params_, pl.dvals, pl.max_w, pl.max_h, 0,
-                       st.count() - 1, s);
+  pl.group_bytes = group_bytes_;
+  return enqueue_range(B, pl.table, params_, group_bytes_, 0, st.count() - 1, s);
 }
 
 void Engine::run(const std::vector<int> &active)
@@ -632,8 +716,7 @@ void Engine::profile(const std::vector<int> &active, float *ms, int *launches)
   LaunchProfile prof;
   try
   {
-    enqueue_range(B, pl.prefix, pl.blocks, params_, pl.dvals, pl.max_w, pl.max_h, 0,
-                  st.count() - 1, stream_, &prof);
+    enqueue_range(B, pl.table, params_, group_bytes_, 0, st.count() - 1, stream_, &prof);
     check(cudaStreamSynchronize(stream_), "profile run");
   }
   catch (...)
@@ -683,8 +766,11 @@ int run_range(const Batch &B, const Shape &s, const qm_params &p, int first, int
               cudaStream_t stream)
 {
   const JobLayout lay = JobLayout::make(s, p.bp_levels);
-  const std::vector<int> blocks = stage_blocks(s, lay, p);
-  return enqueue_range(B, {}, blocks, p, {s.D}, s.W, s.H, first, last, stream);
+  StageTable T;
+  T.add_jobs({stage_blocks(s, lay, p)}, {s.D});
+  T.max_w = s.W;
+  T.max_h = s.H;
+  return enqueue_range(B, T, p, 0, first, last, stream);
 }
 
 int first_of(const char *name, int L)
@@ -696,7 +782,7 @@ int first_of(const char *name, int L)
   if (n == "cost")
     return st.cost();
   if (n == "bp")
-    return L > 1 ? st.pyr(1) : st.mzero();
+    return L > 1 ? st.pyr(1) : st.inherit(0);
   if (n == "upsample")
     return st.row();
   if (n == "fuse")

@@ -179,31 +179,34 @@ __global__ void __launch_bounds__(kFlatThreads)
   reinterpret_cast<float4 *>(Lc.data)[(size_t)cell * D4 + q] = s;
 }
 
-// Messages of the coarsest level start at zero (bpextract.cu:87-90).
-__global__ void __launch_bounds__(kFlatThreads)
-    k_msg_zero(const __grid_constant__ Batch B, int level)
+// The reference's quadtree test of the bp kernel (bpextract.cu:214-220): a
+// cell of level l is left alone by every sweep of that level when the
+// quadtree level at the sample pixel of its pre-checkerboard column (x / 2)
+// exceeds l + 2.
+__device__ __forceinline__ bool bp_skipped(const JobDesc &J, int level, int x, int y, int qt_max)
 {
-  int lb;
-  const JobDesc &J = job_of(B, lb);
-  const LevelDesc &L = J.lv[level];
-  const long n = (long)L.w * L.h * (J.D / 4);
-  const long t = (long)lb * blockDim.x + threadIdx.x;
-  if (t >= n)
-    return;
-#pragma unroll
-  for (int m = 0; m < 4; ++m)
-    reinterpret_cast<float4 *>(L.msg[m])[t] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const int ilev = level + 2;
+  if (ilev > qt_max)
+    return false;
+  const int size = 1 << ilev;
+  const int sx = min((x >> 1) * size, J.W - 1), sy = min(y * size, J.H - 1);
+  return (int)J.levels[(size_t)sy * J.W + sx] > ilev;
 }
 
-// upsample (bpextract.cu:374-395): every cell of level l starts from the
-// message of its parent at level l+1.
+// Message inheritance.  The reference starts every level from a copy of the
+// parent messages (upsample, bpextract.cu:374-395), or from zeros at the
+// coarsest level (bpextract.cu:87-90), and then sweeps.  Most of those copies
+// are never read: the first half-sweep reads the parents directly (the sweep
+// kernel's `first` mode), and every cell the sweeps update overwrites its
+// copy before anyone reads it.  The copies that ARE read later are written
+// here: cells the quadtree test skips at this level, and, with fewer than two
+// iterations, the cells no sweep reaches.
 __global__ void __launch_bounds__(kFlatThreads)
-    k_msg_upsample(const __grid_constant__ Batch B, int level)
+    k_msg_inherit(const __grid_constant__ Batch B, int level, int iters, int qt_max)
 {
   int lb;
   const JobDesc &J = job_of(B, lb);
   const LevelDesc &F = J.lv[level];
-  const LevelDesc &C = J.lv[level + 1];
   const int D4 = J.D / 4;
   const long t = (long)lb * blockDim.x + threadIdx.x;
   if (t >= (long)F.w * F.h * D4)
@@ -211,17 +214,32 @@ __global__ void __launch_bounds__(kFlatThreads)
   const int cell = (int)(t / D4);
   const int q = (int)(t - (long)cell * D4);
   const int x = cell % F.w, y = cell / F.w;
-  const size_t src = ((size_t)(y >> 1) * C.w + (x >> 1)) * D4 + q;
+  // iteration i updates the cells with x + y + i even
+  const bool needed = iters <= 0 || (iters == 1 && ((x + y) & 1)) ||
+                      bp_skipped(J, level, x, y, qt_max);
+  if (!needed)
+    return;
+  if (level + 1 < J.nlev)
+  {
+    const LevelDesc &C = J.lv[level + 1];
+    const size_t src = ((size_t)(y >> 1) * C.w + (x >> 1)) * D4 + q;
 #pragma unroll
-  for (int m = 0; m < 4; ++m)
-    reinterpret_cast<float4 *>(F.msg[m])[t] = reinterpret_cast<const float4 *>(C.msg[m])[src];
+    for (int m = 0; m < 4; ++m)
+      reinterpret_cast<float4 *>(F.msg[m])[t] = reinterpret_cast<const float4 *>(C.msg[m])[src];
+  }
+  else
+  {
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+      reinterpret_cast<float4 *>(F.msg[m])[t] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  }
 }
 
 // ------------------------------------------------------------- sweep
 // bp kernel (bpextract.cu:200-312), one warp per cell of the active colour.
 template <int D, int ARITH>
 __global__ void __launch_bounds__(kCellWarps * 32)
-    k_bp_sweep(const __grid_constant__ Batch B, int level, int parity, KParams kp)
+    k_bp_sweep(const __grid_constant__ Batch B, int level, int parity, int first, KParams kp)
 {
   constexpr int NV = HypLayout<D>::NV;
   int lb;
@@ -235,20 +253,33 @@ __global__ void __launch_bounds__(kCellWarps * 32)
   if (warp >= hw * h)
     return;
   const int y = warp / hw, bx = warp - y * hw;
-  // quadtree skip test on the pre-checkerboard column (bpextract.cu:214-220)
-  const int ilev = level + 2;
-  if (ilev <= kp.qt_max)
-  {
-    const int size = 1 << ilev;
-    const int sx = min(bx * size, J.W - 1), sy = min(y * size, J.H - 1);
-    if ((int)J.levels[(size_t)sy * J.W + sx] > ilev)
-      return;
-  }
-  const int x = 2 * bx + ((y + parity) & 1);
-  if (x >= w)
+  const int x = 2 * bx + ((y + parity) & 1); // bx == x / 2
+  if (x >= w || bp_skipped(J, level, x, y, kp.qt_max))
     return;
   const bool has_u = y > 0, has_d = y < h - 1, has_l = x > 0, has_r = x < w - 1;
   const size_t c = (size_t)y * w + x;
+
+  // Incoming messages: the neighbours' own ones, or in the first half-sweep
+  // of a level the ones their parents ended with (0 at the coarsest level),
+  // which is what the reference's copied-down messages hold at that point.
+  const float *src_u = nullptr, *src_d = nullptr, *src_l = nullptr, *src_r = nullptr;
+  if (!first)
+  {
+    src_u = L.msg[kDown] + (c - w) * D;
+    src_d = L.msg[kUp] + (c + w) * D;
+    src_l = L.msg[kRight] + (c - 1) * D;
+    src_r = L.msg[kLeft] + (c + 1) * D;
+  }
+  else if (level + 1 < J.nlev)
+  {
+    const LevelDesc &C = J.lv[level + 1];
+    auto parent = [&](int xn, int yn) { return ((size_t)(yn >> 1) * C.w + (xn >> 1)) * D; };
+    src_u = C.msg[kDown] + parent(x, y - 1);
+    src_d = C.msg[kUp] + parent(x, y + 1);
+    src_l = C.msg[kRight] + parent(x - 1, y);
+    src_r = C.msg[kLeft] + parent(x + 1, y);
+  }
+  const bool ld = src_u != nullptr;
 
   float dat[NV], fu[NV], fd[NV], fl[NV], fr[NV];
 #pragma unroll
@@ -257,10 +288,10 @@ __global__ void __launch_bounds__(kCellWarps * 32)
     const int d = lane + 32 * k;
     const bool in = d < D;
     dat[k] = in ? L.data[c * D + d] : 0.0f;
-    fu[k] = (in && has_u) ? L.msg[kDown][(c - w) * D + d] : 0.0f;
-    fd[k] = (in && has_d) ? L.msg[kUp][(c + w) * D + d] : 0.0f;
-    fl[k] = (in && has_l) ? L.msg[kRight][(c - 1) * D + d] : 0.0f;
-    fr[k] = (in && has_r) ? L.msg[kLeft][(c + 1) * D + d] : 0.0f;
+    fu[k] = (in && ld && has_u) ? src_u[d] : 0.0f;
+    fd[k] = (in && ld && has_d) ? src_d[d] : 0.0f;
+    fl[k] = (in && ld && has_l) ? src_l[d] : 0.0f;
+    fr[k] = (in && ld && has_r) ? src_r[d] : 0.0f;
   }
   const float P1 = kp.P1, P2 = kp.P2;
 #pragma unroll
@@ -419,14 +450,15 @@ __global__ void __launch_bounds__(kCellWarps * 32)
 }
 
 template <int D>
-void sweep_d(const Batch &B, int blocks, int level,
-             int parity, KParams kp, int arith, cudaStream_t s)
+void sweep_d(const Batch &B, int blocks, int level, int it, KParams kp, int arith,
+             cudaStream_t s)
 {
+  const int parity = it & 1, first = it == 0 ? 1 : 0;
   if (arith == QM_ARITH_IEEE)
-    k_bp_sweep<D, QM_ARITH_IEEE><<<blocks, kCellWarps * 32, 0, s>>>(B, level,
-                                                                     parity, kp);
+    k_bp_sweep<D, QM_ARITH_IEEE><<<blocks, kCellWarps * 32, 0, s>>>(B, level, parity, first, kp);
   else
-    k_bp_sweep<D, QM_ARITH_REFERENCE><<<blocks, kCellWarps * 32, 0, s>>>(B, level, parity, kp);
+    k_bp_sweep<D, QM_ARITH_REFERENCE><<<blocks, kCellWarps * 32, 0, s>>>(B, level, parity, first,
+                                                                         kp);
 }
 
 template <int D>
@@ -449,30 +481,24 @@ void launch_pyramid(const Batch &B, int blocks, int level,
   k_pyramid<<<blocks, kFlatThreads, 0, s>>>(B, level);
 }
 
-void launch_msg_zero(const Batch &B, int blocks, int level,
-                     cudaStream_t s)
+void launch_msg_inherit(const Batch &B, int blocks, int level, int iters, int qt_max,
+                        cudaStream_t s)
 {
-  k_msg_zero<<<blocks, kFlatThreads, 0, s>>>(B, level);
-}
-
-void launch_msg_upsample(const Batch &B, int blocks, int level,
-                         cudaStream_t s)
-{
-  k_msg_upsample<<<blocks, kFlatThreads, 0, s>>>(B, level);
+  k_msg_inherit<<<blocks, kFlatThreads, 0, s>>>(B, level, iters, qt_max);
 }
 
 // A batch with mixed hypothesis counts launches one sweep per count present;
 // each launch skips the jobs of other counts.
-void launch_bp_sweep(const Batch &B, int blocks, int d,
-                     int level, int parity, KParams kp, int arith, cudaStream_t s)
+void launch_bp_sweep(const Batch &B, int blocks, int d, int level, int it, KParams kp, int arith,
+                     cudaStream_t s)
 {
   switch (d)
   {
-  case 32: sweep_d<32>(B, blocks, level, parity, kp, arith, s); break;
-  case 48: sweep_d<48>(B, blocks, level, parity, kp, arith, s); break;
-  case 64: sweep_d<64>(B, blocks, level, parity, kp, arith, s); break;
-  case 96: sweep_d<96>(B, blocks, level, parity, kp, arith, s); break;
-  case 128: sweep_d<128>(B, blocks, level, parity, kp, arith, s); break;
+  case 32: sweep_d<32>(B, blocks, level, it, kp, arith, s); break;
+  case 48: sweep_d<48>(B, blocks, level, it, kp, arith, s); break;
+  case 64: sweep_d<64>(B, blocks, level, it, kp, arith, s); break;
+  case 96: sweep_d<96>(B, blocks, level, it, kp, arith, s); break;
+  case 128: sweep_d<128>(B, blocks, level, it, kp, arith, s); break;
   default: break;
   }
 }

@@ -27,15 +27,34 @@ namespace qm
 namespace
 {
 
-// floor(u + 0.5) for 0 <= u + 0.5 < 2^23 with two round-down additions: the
-// largest float <= u + 0.5 has the same floor as u + 0.5 (integers are
-// floats), and adding 2^23 rounded down leaves exactly 2^23 + floor in the
-// float, whose bit pattern minus that of 2^23 is the integer.  This equals the
-// reference's (int)((double)u + 0.5) on that range.
-__device__ __forceinline__ int round_half_up(float u)
+// floor(c + 0.5) for -0.5 <= c < 2^22 - 0.5, which equals the reference's
+// (int)((double)c + 0.5) there, as HALF the integer n = floor(2c + 1): the
+// sum c + (2^22 + 0.5) lies in [2^22, 2^23), where floats are spaced 0.5
+// apart, so rounding it down gives 2^22 + n/2 exactly, and the bit pattern of
+// that float minus the one of 2^22 is n.  The caller shifts right by one.
+// The returned value is the bit pattern itself; kHalfBias = bits(2^22) / 2 is
+// subtracted (folded into the image offset) after the shift.
+__device__ __forceinline__ unsigned twice_round_bits(float c)
 {
-  const float f = __fadd_rd(__fadd_rd(u, 0.5f), 8388608.0f);
-  return __float_as_int(f) - 0x4B000000;
+  return (unsigned)__float_as_int(__fadd_rd(c, 4194304.5f));
+}
+constexpr unsigned kHalfBias = 0x4A800000u >> 1;
+
+// The 3x3 patch coordinates along one axis.  The reference computes
+// (u + a*i) + b*j for i, j in {-1, 0, 1} (i the patch column, j the row).
+// The products are exact (a*(+-1) = +-a, a*0 = +-0, and c +- 0 = c), so in
+// both arithmetic modes the nine values are these correctly rounded sums:
+// three column bases, then three rows each.  c[3*(j+1) + (i+1)].
+__device__ __forceinline__ void patch_axis(float u, float a, float b, float (&c)[9])
+{
+  const float r[3] = {__fadd_rn(u, -a), u, __fadd_rn(u, a)};
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+  {
+    c[i] = __fadd_rn(r[i], -b);
+    c[3 + i] = r[i];
+    c[6 + i] = __fadd_rn(r[i], b);
+  }
 }
 
 template <class A>
@@ -91,6 +110,7 @@ __global__ void __launch_bounds__(kFlatThreads)
   // (int)(u + 0.5) in [2, W-2) exactly when u in [1.5, W-2.5) (both bounds
   // are floats, the comparisons exact; NaN fails)
   const float ulo = 1.5f, uhi = (float)W - 2.5f, vhi = (float)H - 2.5f;
+  const unsigned bias = 0u - kHalfBias * ((unsigned)pitch + 1u);
   int sad = 0, nvalid = 0;
   for (int f = 0; f < F; ++f)
   {
@@ -104,20 +124,23 @@ __global__ void __launch_bounds__(kFlatThreads)
     if (uv.x >= ulo && uv.x < uhi && uv.y >= ulo && uv.y < vhi)
     {
       const uint8_t *m = s_img[f];
-      const float u2u = T[0], u2v = T[4], v2u = T[1], v2v = T[5];
       // The slot poses are validated as rigid on the host (|r00|+|r01| and
       // |r10|+|r11| <= 1.5), so every patch coordinate + 0.5 lies in
       // [0.5, W-0.5) x [0.5, H-0.5): no clamp needed.
+      float px[9], py[9];
+      patch_axis(uv.x, T[0], T[1], px);
+      patch_axis(uv.y, T[4], T[5], py);
       unsigned s = 0;
 #pragma unroll
-      for (int jj = -1; jj <= 1; ++jj)
-#pragma unroll
-        for (int ii = -1; ii <= 1; ++ii)
-        {
-          const int chx = round_half_up(A::patch_coord(uv.x, u2u, ii, v2u, jj));
-          const int chy = round_half_up(A::patch_coord(uv.y, u2v, ii, v2v, jj));
-          s = __usad((unsigned)patch[ii + 1][jj + 1], (unsigned)__ldg(m + chy * pitch + chx), s);
-        }
+      for (int k = 0; k < 9; ++k)
+      {
+        // offset = floor(py+0.5)*pitch + floor(px+0.5), in 32-bit wrap-around
+        // arithmetic (the true offset is below 2^31)
+        const unsigned hx = twice_round_bits(px[k]) >> 1;
+        const unsigned hy = twice_round_bits(py[k]) >> 1;
+        const unsigned off = hy * (unsigned)pitch + hx + bias;
+        s = __usad((unsigned)patch[k % 3][k / 3], (unsigned)__ldg(m + off), s);
+      }
       const int wgt = s_w[f];
       sad += wgt * (int)s;
       nvalid += wgt;

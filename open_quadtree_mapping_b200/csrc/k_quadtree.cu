@@ -109,13 +109,128 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// Summary of an aligned block: intensity sum, max, min, and whether it is
+// complete (inside the image) with every sub-block approved.
+struct Node
+{
+  int sum, mx, mn;
+  bool ok;
+};
+
+__device__ __forceinline__ Node merge(Node a, Node b)
+{
+  return Node{a.sum + b.sum, max(a.mx, b.mx), min(a.mn, b.mn), a.ok && b.ok};
+}
+
+__device__ __forceinline__ Node merge_lane(Node a, int lane_xor)
+{
+  Node b;
+  b.sum = __shfl_xor_sync(0xffffffffu, a.sum, lane_xor);
+  b.mx = __shfl_xor_sync(0xffffffffu, a.mx, lane_xor);
+  b.mn = __shfl_xor_sync(0xffffffffu, a.mn, lane_xor);
+  b.ok = __shfl_xor_sync(0xffffffffu, a.ok ? 1 : 0, lane_xor) != 0;
+  return merge(a, b);
+}
+
+// approval of a complete block of 4^i pixels (same arithmetic as above)
+__device__ __forceinline__ bool approve(const Node &n, int i, float thr)
+{
+  if (!n.ok)
+    return false;
+  const float mean = (float)n.sum * (1.0f / (float)(1 << (2 * i)));
+  return ((float)n.mx - mean <= thr) && (mean - (float)n.mn <= thr);
+}
+
+constexpr int kQtWarps = 8;
+
+// The default 16 x 16 tile (qt_max = 4), one warp per tile and no shared
+// memory: lane (a, b) = (lane & 3, lane >> 2) owns the 4 x 2 pixels at
+// columns 4a..4a+3, rows 2b, 2b+1 -- two 2x2 blocks of level 1.  Level 2
+// joins lanes b ^ 1 (lane ^ 4), level 3 lanes a ^ 1 and b ^ 2 (lane ^ 1,
+// ^ 8), level 4 lanes a ^ 2 and b ^ 4 (lane ^ 2, ^ 16).  Results equal the
+// general kernel's (integer sums and extrema, the same float test).
+__global__ void __launch_bounds__(kQtWarps * 32)
+    k_quadtree16(const __grid_constant__ Batch B, KParams kp)
+{
+  int lb;
+  const JobDesc &J = job_of(B, lb);
+  const int W = J.W, H = J.H;
+  const int tiles_x = (W + 15) >> 4;
+  const int tile = lb * kQtWarps + (threadIdx.x >> 5);
+  if (tile >= tiles_x * ((H + 15) >> 4))
+    return;
+  const int lane = threadIdx.x & 31, a = lane & 3, b = lane >> 2;
+  const int x0 = (tile % tiles_x) * 16 + 4 * a, y0 = (tile / tiles_x) * 16 + 2 * b;
+  int v[2][4];
+  bool in[2][4];
+#pragma unroll
+  for (int r = 0; r < 2; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+    {
+      in[r][c] = x0 + c < W && y0 + r < H;
+      v[r][c] = in[r][c] ? (int)J.ref[(size_t)(y0 + r) * J.ref_pitch + x0 + c] : 0;
+    }
+  // level 1: the lane's two 2x2 blocks
+  Node n1[2];
+  bool ok1[2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k)
+  {
+    Node n{0, 0, 255, true};
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+      for (int c = 2 * k; c < 2 * k + 2; ++c)
+      {
+        n.sum += v[r][c];
+        n.mx = max(n.mx, v[r][c]);
+        n.mn = min(n.mn, v[r][c]);
+        n.ok = n.ok && in[r][c];
+      }
+    ok1[k] = approve(n, 1, kp.qt_thr);
+    n1[k] = Node{n.sum, n.mx, n.mn, ok1[k]};
+  }
+  Node n2 = merge(n1[0], n1[1]);
+  n2 = merge_lane(n2, 4);
+  const bool ok2 = approve(n2, 2, kp.qt_thr);
+  n2.ok = ok2;
+  Node n3 = merge_lane(merge_lane(n2, 1), 8);
+  const bool ok3 = approve(n3, 3, kp.qt_thr);
+  n3.ok = ok3;
+  Node n4 = merge_lane(merge_lane(n3, 2), 16);
+  const bool ok4 = approve(n4, 4, kp.qt_thr);
+  const int upper = ok4 ? 4 : ok3 ? 3 : ok2 ? 2 : 1;
+#pragma unroll
+  for (int r = 0; r < 2; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+    {
+      if (!in[r][c])
+        continue;
+      const int level = ok1[c >> 1] ? upper : 0;
+      const size_t o = (size_t)(y0 + r) * W + x0 + c;
+      J.levels[o] = (uint8_t)max(level, kp.qt_min);
+      if (J.sparse)
+        J.sparse[o] = 0.0f; // the debug image starts empty
+    }
+}
+
 } // namespace
 
-int quadtree_tile(int qt_max) { return 1 << qt_max; }
+int quadtree_blocks(int W, int H, int qt_max)
+{
+  const int T = 1 << qt_max;
+  const int tiles = ((W + T - 1) / T) * ((H + T - 1) / T);
+  return qt_max == 4 ? (tiles + kQtWarps - 1) / kQtWarps : tiles;
+}
 
 void launch_quadtree(const Batch &B, int blocks, KParams kp, cudaStream_t s)
 {
-  k_quadtree<<<blocks, 256, 0, s>>>(B, kp);
+  if (kp.qt_max == 4)
+    k_quadtree16<<<blocks, kQtWarps * 32, 0, s>>>(B, kp);
+  else
+    k_quadtree<<<blocks, 256, 0, s>>>(B, kp);
 }
 
 } // namespace qm

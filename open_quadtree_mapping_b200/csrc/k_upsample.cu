@@ -44,7 +44,9 @@ namespace qm
 namespace
 {
 
-constexpr int kArrays = 6; // w, rd, ri, cp, dd (holds 1/den first), di
+// per line: w (weights, then alpha), rd / ri (right-hand sides, then the
+// scaled right-hand sides, the forward values and the solution), cp (pivots)
+constexpr int kArrays = 4;
 
 __host__ __device__ __forceinline__ int seg_len(int n) { return (n + 31) / 32; }
 __host__ __device__ __forceinline__ int seg_pitch(int n) { return seg_len(n) | 1; }
@@ -53,7 +55,7 @@ __host__ __device__ __forceinline__ int line_floats(int n) { return 32 * seg_pit
 
 struct LineBuf
 {
-  float *w, *rd, *ri, *cp, *dd, *di;
+  float *w, *rd, *ri, *cp;
   int n, m, mp;
   __device__ __forceinline__ int pos(int k) const
   {
@@ -70,8 +72,6 @@ __device__ __forceinline__ LineBuf line_buf(float *base, int n)
   b.rd = base + L;
   b.ri = base + 2 * L;
   b.cp = base + 3 * L;
-  b.dd = base + 4 * L;
-  b.di = base + 5 * L;
   b.n = n;
   b.m = seg_len(n);
   b.mp = seg_pitch(n);
@@ -122,13 +122,18 @@ struct Aff
 };
 
 // Solves the line held in `b` (w, rd, ri filled) and leaves the solution in
-// dd (depth) and di (indicator).  Whole warp.
+// rd (depth) and ri (indicator).  Whole warp.  Every element is rewritten in
+// place by the lane that owns it, except w[e] (the first weight of the next
+// segment), which each lane reads before the pass that overwrites w.
 __device__ void solve_line(const LineBuf &b, double lam)
 {
   const int lane = threadIdx.x & 31;
   const int s = min(lane * b.m, b.n);
   const int e = min(s + b.m, b.n);
   const int base = lane * b.mp; // smem position of element s
+  // right weight of the segment's last element
+  const float w_end = b.w[e < b.n ? b.pos(e) : 32 * b.mp];
+  __syncwarp();
   // -------- pivots: segment Moebius product (apply element s first).  The
   // entries grow by at most 1 + 2*lambda per element, far inside the double
   // range for segments of <= 128 elements, so no per-step rescaling.
@@ -137,7 +142,7 @@ __device__ void solve_line(const LineBuf &b, double lam)
   {
     const int p = base + (k - s);
     const double wl = b.w[p];
-    const double wr = b.w[k + 1 < b.n ? b.pos(k + 1) : 32 * b.mp];
+    const double wr = k + 1 < e ? b.w[p + 1] : w_end;
     const double a = -lam * wl, bb = 1.0 + lam * (wl + wr), c = -lam * wr;
     P = Mat2{c * P.c, c * P.d, bb * P.c - a * P.a, bb * P.d - a * P.b};
   }
@@ -159,6 +164,8 @@ __device__ void solve_line(const LineBuf &b, double lam)
   // (Q.a z0 + Q.b) / D_k where D_k = Q.c z0 + Q.d, and den_k = D_k / D_{k-1},
   // so 1/den_k = D_{k-1} / D_k and c'_k = c_k / den_k.  Only the 2x2 products
   // form the serial chain; the one division per element does not feed back.
+  // The forward recurrence d'_k = alpha_k d'_{k-1} + r_k / den_k keeps
+  // alpha_k = -a_k / den_k (in w) and r_k / den_k (in rd, ri).
   Mat2 Q{1.0, 0.0, 0.0, 1.0};
   double Dprev = 1.0;
   Aff F{1.0f, 0.0f, 0.0f};
@@ -166,19 +173,20 @@ __device__ void solve_line(const LineBuf &b, double lam)
   {
     const int p = base + (k - s);
     const double wl = b.w[p];
-    const double wr = b.w[k + 1 < b.n ? b.pos(k + 1) : 32 * b.mp];
+    const double wr = k + 1 < e ? b.w[p + 1] : w_end;
     const double a = -lam * wl, bb = 1.0 + lam * (wl + wr), c = -lam * wr;
     Q = Mat2{c * Q.c, c * Q.d, bb * Q.c - a * Q.a, bb * Q.d - a * Q.b};
     const double Dk = Q.c * z0 + Q.d;
     const double inv = Dprev / Dk; // 1 / den_k
     Dprev = Dk;
-    const double cp = c * inv;
-    b.cp[p] = (float)cp;
+    b.cp[p] = (float)(c * inv);
     const float invf = (float)inv;
-    b.dd[p] = invf;
-    // alpha_k = -a_k / den_k, formed the same way in both passes below
     const float alpha = (float)(lam * wl) * invf;
-    F = Aff{alpha * F.g, alpha * F.hd + b.rd[p] * invf, alpha * F.hi + b.ri[p] * invf};
+    const float qd = b.rd[p] * invf, qi = b.ri[p] * invf;
+    b.w[p] = alpha;
+    b.rd[p] = qd;
+    b.ri[p] = qi;
+    F = Aff{alpha * F.g, alpha * F.hd + qd, alpha * F.hi + qi};
   }
 #pragma unroll
   for (int off = 1; off < 32; off <<= 1)
@@ -198,12 +206,11 @@ __device__ void solve_line(const LineBuf &b, double lam)
   for (int k = s; k < e; ++k)
   {
     const int p = base + (k - s);
-    const float invf = b.dd[p];
-    const float alpha = (float)(lam * (double)b.w[p]) * invf;
-    dprev = alpha * dprev + b.rd[p] * invf;
-    iprev = alpha * iprev + b.ri[p] * invf;
-    b.dd[p] = dprev;
-    b.di[p] = iprev;
+    const float alpha = b.w[p];
+    dprev = alpha * dprev + b.rd[p];
+    iprev = alpha * iprev + b.ri[p];
+    b.rd[p] = dprev;
+    b.ri[p] = iprev;
     const float cpk = b.cp[p];
     G = Aff{-G.g * cpk, G.g * dprev + G.hd, G.g * iprev + G.hi};
   }
@@ -226,10 +233,10 @@ __device__ void solve_line(const LineBuf &b, double lam)
   {
     const int p = base + (k - s);
     const float cpk = b.cp[p];
-    zd = b.dd[p] - cpk * zd;
-    zi = b.di[p] - cpk * zi;
-    b.dd[p] = zd;
-    b.di[p] = zi;
+    zd = b.rd[p] - cpk * zd;
+    zi = b.ri[p] - cpk * zi;
+    b.rd[p] = zd;
+    b.ri[p] = zi;
   }
   __syncwarp();
 }
@@ -268,7 +275,7 @@ __global__ void __launch_bounds__(kRowWarps * 32)
   for (int k = lane; k < n; k += 32)
   {
     const int p = b.pos(k);
-    out[k] = make_float2(b.dd[p], b.di[p]);
+    out[k] = make_float2(b.rd[p], b.ri[p]);
   }
 }
 
@@ -317,7 +324,7 @@ __global__ void __launch_bounds__(kColLines * 32)
       continue;
     LineBuf b = line_buf(smem + c * per_line, n);
     const int p = b.pos(k);
-    J.dense[(size_t)k * W + x] = A::div(b.dd[p], b.di[p]);
+    J.dense[(size_t)k * W + x] = A::div(b.rd[p], b.ri[p]);
   }
 }
 

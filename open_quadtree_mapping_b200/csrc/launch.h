@@ -25,17 +25,21 @@ size_t row_solve_smem(int max_w);
 size_t col_solve_smem(int max_h);
 void prepare_upsample_kernels();
 
-int quadtree_tile(int qt_max);
+// blocks of the quadtree launch for one W x H image
+int quadtree_blocks(int W, int H, int qt_max);
 
 // Every launcher takes the batch by value (the kernels receive it as a
 // __grid_constant__ parameter); B.prefix must point at the stage's prefix.
 void launch_quadtree(const Batch &B, int blocks, KParams kp, cudaStream_t s);
 void launch_cost(const Batch &B, int blocks, int arith, cudaStream_t s);
 void launch_pyramid(const Batch &B, int blocks, int level, cudaStream_t s);
-void launch_msg_zero(const Batch &B, int blocks, int level, cudaStream_t s);
-void launch_msg_upsample(const Batch &B, int blocks, int level, cudaStream_t s);
-void launch_bp_sweep(const Batch &B, int blocks, int d, int level, int parity, KParams kp,
-                     int arith, cudaStream_t s);
+// writes the inherited messages of level `level` that its sweeps will read
+// (cells the quadtree test skips; all unswept cells when iters < 2)
+void launch_msg_inherit(const Batch &B, int blocks, int level, int iters, int qt_max,
+                        cudaStream_t s);
+// half-sweep `it` (0-based) of level `level`
+void launch_bp_sweep(const Batch &B, int blocks, int d, int level, int it, KParams kp, int arith,
+                     cudaStream_t s);
 void launch_extract(const Batch &B, int blocks, int d, int arith, cudaStream_t s);
 void launch_row_solve(const Batch &B, int blocks, KParams kp, int arith, int max_w,
                       cudaStream_t s);

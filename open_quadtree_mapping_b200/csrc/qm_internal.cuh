@@ -92,6 +92,8 @@ struct Batch
   const JobDesc *jobs; // null: the single job `one`
   const int *prefix;   // block prefix of this stage over the jobs
   int njobs;
+  int block0;  // global block index of this launch's first block (job groups)
+  int uniform; // > 0: every job has this many blocks (job = block / uniform)
   const uint8_t *const *slot_ptr; // per slot, device image (null: `slots`)
   const float *slot_T;            // per slot, 12 floats T_slot<-ref
   const int *slot_w;              // per slot, multiplicity
@@ -122,16 +124,24 @@ __device__ __forceinline__ int find_job(const int *__restrict__ prefix, int njob
   return lo;
 }
 
-// The job of this block and the block's index inside that job.
+// The job of this block and the block's index inside that job.  A launch may
+// cover a contiguous group of jobs only: its blocks then start at block0.
 __device__ __forceinline__ const JobDesc &job_of(const Batch &B, int &local_block)
 {
+  const int block = (int)blockIdx.x + B.block0;
   if (B.jobs == nullptr)
   {
-    local_block = blockIdx.x;
+    local_block = block;
     return B.one;
   }
-  const int j = find_job(B.prefix, B.njobs, blockIdx.x);
-  local_block = blockIdx.x - __ldg(B.prefix + j);
+  if (B.uniform > 0)
+  {
+    const int j = block / B.uniform;
+    local_block = block - j * B.uniform;
+    return B.jobs[j];
+  }
+  const int j = find_job(B.prefix, B.njobs, block);
+  local_block = block - __ldg(B.prefix + j);
   return B.jobs[j];
 }
 
@@ -194,10 +204,6 @@ struct ArithRef
   {
     return 1.0 / (step * d + mn);
   }
-  static __device__ __forceinline__ float patch_coord(float base, float a, int i, float b, int j)
-  {
-    return base + a * i + b * j;
-  }
   // my_depth_cost / (float)aggregate_num / 255.0f (depth_extract.cu:223)
   static __device__ __forceinline__ float sad_norm(float sad, float n) { return sad / n / 255.0f; }
   static __device__ __forceinline__ float length(float3 p) { return sqrtf(p.x * p.x + p.y * p.y + p.z * p.z); }
@@ -239,10 +245,6 @@ struct ArithIeee
   static __device__ __forceinline__ float hyp_depth(double step, double mn, int d)
   {
     return (float)__ddiv_rn(1.0, __dadd_rn(__dmul_rn(step, (double)d), mn));
-  }
-  static __device__ __forceinline__ float patch_coord(float base, float a, int i, float b, int j)
-  {
-    return __fadd_rn(__fadd_rn(base, __fmul_rn(a, (float)i)), __fmul_rn(b, (float)j));
   }
   static __device__ __forceinline__ float sad_norm(float sad, float n)
   {

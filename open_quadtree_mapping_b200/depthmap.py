@@ -190,6 +190,10 @@ class BatchDepthmap:
     def set_graphs(self, on: bool) -> None:
         _lib.check(_lib.lib().qm_batch_set_graphs(self._h, 1 if on else 0))
 
+    def set_group_bytes(self, nbytes: int) -> None:
+        """L2 budget of a BP job range (0 = all streams at once)."""
+        _lib.check(_lib.lib().qm_batch_set_group_bytes(self._h, int(nbytes)))
+
     def last_launches(self) -> int:
         c = ctypes.c_int()
         _lib.check(_lib.lib().qm_batch_last_launches(self._h, ctypes.byref(c)))

@@ -78,18 +78,27 @@ def test_batch_equals_plain_and_graph_equals_eager(gpu):
     batch = BatchDepthmap([_stream_kw()] * 3, params=p)
     eager = BatchDepthmap([_stream_kw()] * 3, params=p)
     eager.set_graphs(False)
+    # BP job ranges: one stream per range, and all streams in one range
+    split = BatchDepthmap([_stream_kw()] * 3, params=p)
+    split.set_group_bytes(1)
+    whole = BatchDepthmap([_stream_kw()] * 3, params=p)
+    whole.set_group_bytes(0)
     singles = [BatchDepthmap([_stream_kw()], params=p) for _ in range(3)]
     for i in range(14):
         imgs = [s[0][i] for s in seqs]
         poses = [s[1][i] for s in seqs]
         hb = batch.add_frames(imgs, poses)
         he = eager.add_frames(imgs, poses)
+        assert split.add_frames(imgs, poses) == hb
+        assert whole.add_frames(imgs, poses) == hb
         hs = [singles[k].add_frames([imgs[k]], [poses[k]])[0] for k in range(3)]
         assert hb == he == hs
         if all(hb) and i > 0:
             for k in range(3):
                 a = batch.get_depth(k)
                 assert np.array_equal(a, eager.get_depth(k))
+                assert np.array_equal(a, split.get_depth(k))
+                assert np.array_equal(a, whole.get_depth(k))
                 assert np.array_equal(a, singles[k].get_depth(0))
                 assert np.array_equal(batch.get_debug(k), singles[k].get_debug(0))
     assert batch.last_launches() > 0
@@ -104,6 +113,7 @@ def test_uneven_batch_equals_per_stream(gpu):
     descs = [_stream_kw(W=w, H=h, f=460.0 * w / 752.0, num_hyp=d, num_slots=f)
              for (w, h, d, f) in shapes]
     batch = BatchDepthmap(descs, params=p)
+    batch.set_group_bytes(3 << 20)  # ranges of one or two streams
     singles = [BatchDepthmap([d], params=p) for d in descs]
     for i in range(13):
         imgs = [s[0][i] for s in seqs]
