@@ -57,7 +57,7 @@ std::vector<int> stage_blocks(const Shape &s, const JobLayout &lay, const qm_par
   const int L = p.bp_levels;
   const int D = s.D;
   b[st.qt()] = quadtree_blocks(s.W, s.H, p.qt_max_level);
-  b[st.cost()] = cdiv((long)lay.lw[0] * lay.lh[0] * D, kFlatThreads);
+  b[st.cost()] = cost_blocks(lay.lw[0], lay.lh[0]);
   // pyramid and message kernels move float4 groups of hypotheses
   for (int l = 1; l < L; ++l)
     b[st.pyr(l)] = cdiv((long)lay.lw[l] * lay.lh[l] * (D / 4), kFlatThreads);
@@ -176,7 +176,8 @@ int enqueue_range(const Batch &B, const StageTable &T, const qm_params &p, size_
       launch(kind, [&] { fn(b, grid); });
   };
   all(kQuadtree, st.qt(), [&](const Batch &b, int g) { launch_quadtree(b, g, kp, s); });
-  all(kCost, st.cost(), [&](const Batch &b, int g) { launch_cost(b, g, ar, s); });
+  const int max_d = T.dvals.empty() ? 0 : T.dvals.back();
+  all(kCost, st.cost(), [&](const Batch &b, int g) { launch_cost(b, g, ar, max_d, s); });
   for (int l = 1; l < L; ++l)
     all(kPyramid, st.pyr(l), [&](const Batch &b, int g) { launch_pyramid(b, g, l, s); });
   // BP, coarse to fine; each level runs job range by job range (message

@@ -1,13 +1,18 @@
 // Multi-view matching cost at quadtree nodes (image_to_cost +
 // normalize_the_cost, depth_extract.cu:135-244 of the reference).
 //
-// One thread per (cell, hypothesis); consecutive threads are consecutive
-// hypotheses of a cell, so the cost row of a cell (the PIXEL_COST layout,
-// hypotheses contiguous) is written coalesced.  Each thread loops over the
-// measurement slots itself and accumulates the 3x3 SAD as an integer: every
-// term is an integer intensity difference, so the sum is exact and equal to
-// the reference's shared-memory tree over slots.  The projection follows the
-// reference's arithmetic (ArithRef) or IEEE rounding (ArithIeee).
+// A block owns a tile of kCostCells consecutive cells of one cell row.  Warp
+// 0 finds the tile's node cells (ballot) and stages, per node, its ray and
+// 3x3 reference patch in shared memory; the block also stages the slot poses
+// and the hypothesis depths.  The block's threads then take the (node,
+// hypothesis) pairs node-fastest, so the lanes of a warp evaluate
+// neighbouring nodes at one depth: their projections are neighbours in the
+// slot image and a gather touches few cache lines.  Each pair loops over the
+// measurement slots and accumulates the 3x3 SAD as an integer: every term is
+// an integer intensity difference, so the sum is exact and equal to the
+// reference's shared-memory tree over slots.  The projection follows the
+// reference's arithmetic (ArithRef) or IEEE rounding (ArithIeee).  The tile's
+// costs are assembled in shared memory and written as one contiguous run.
 //
 // Cells that are not node origins, or touch the border (x <= 0, y <= 0,
 // x >= W-1, y >= H-1), get cost 0 for every hypothesis, as the reference's
@@ -61,104 +66,152 @@ template <class A>
 __global__ void __launch_bounds__(kFlatThreads)
     k_cost(const __grid_constant__ Batch B)
 {
+  // costs of the tile, [kCostCells][D + 1] (the padding keeps lanes that
+  // store one hypothesis of different cells on different banks)
+  extern __shared__ float s_out[];
   __shared__ float4 s_pose[kMaxSlots * 3];
   __shared__ const uint8_t *s_img[kMaxSlots];
   __shared__ int s_w[kMaxSlots];
+  __shared__ float s_depth[kMaxHyp];
+  // node cells of the tile, in x order: tile column, ray, 3x3 patch
+  __shared__ int s_col[kCostCells];
+  __shared__ float s_dir[3][kCostCells];
+  __shared__ int s_patch[9][kCostCells];
+  __shared__ int s_nodes;
   int lb;
   const JobDesc &J = job_of(B, lb);
-  const int D = J.D;
-  const int F = J.F;
-  // the job's (deduplicated) slots, staged once per block; every block
-  // belongs to one job
-  for (int i = threadIdx.x; i < F * 12; i += blockDim.x)
+  const int D = J.D, F = J.F, W = J.W, H = J.H;
+  const int segs = (J.cw + kCostCells - 1) / kCostCells;
+  const int cy = lb / segs, cx0 = (lb - cy * segs) * kCostCells;
+  const int ncells = min(kCostCells, J.cw - cx0);
+  const int tid = threadIdx.x;
+  // the job's (deduplicated) slots and the hypothesis depths, once per block
+  for (int i = tid; i < F * 12; i += blockDim.x)
     reinterpret_cast<float *>(s_pose)[i] = slot_pose(B, J.slot_base + i / 12)[i % 12];
-  for (int i = threadIdx.x; i < F; i += blockDim.x)
+  for (int i = tid; i < F; i += blockDim.x)
   {
     s_img[i] = slot_image(B, J.slot_base + i);
     s_w[i] = slot_weight(B, J.slot_base + i);
   }
-  __syncthreads();
-  const long t = (long)lb * blockDim.x + threadIdx.x;
-  const int ncell = J.cw * J.ch;
-  if (t >= (long)ncell * D)
-    return;
-  const int cell = (int)(t / D);
-  const int d = (int)(t - (long)cell * D);
-  const int cx = cell % J.cw, cy = cell / J.cw;
-  const int x = cx * 4, y = cy * 4;
-  const int W = J.W, H = J.H;
-  float *out = J.lv[0].data + (size_t)cell * D + d;
-  const int size = 1 << J.levels[(size_t)y * W + x];
-  if (x >= W - 1 || y >= H - 1 || x <= 0 || y <= 0 || x % size != 0 || y % size != 0)
-  {
-    *out = 0.0f;
-    return;
-  }
-  int patch[3][3];
-  const uint8_t *r = J.ref + (size_t)(y - 1) * J.ref_pitch + (x - 1);
-#pragma unroll
-  for (int jj = 0; jj < 3; ++jj)
-#pragma unroll
-    for (int ii = 0; ii < 3; ++ii)
-      patch[ii][jj] = __ldg(r + (size_t)jj * J.ref_pitch + ii);
-
+  for (int d = tid; d < D; d += blockDim.x)
+    s_depth[d] = A::hyp_depth(J.step, J.min_inv, d);
+  const int sd = D + 1;
+  for (int i = tid; i < ncells * sd; i += blockDim.x)
+    s_out[i] = 0.0f;
   const Cam cam{J.fx, J.fy, J.cx, J.cy};
-  const float3 dir = A::ray((float)x, (float)y, cam);
-  const float depth = A::hyp_depth(J.step, J.min_inv, d);
-  const float3 p = A::scale(dir, depth);
+  if (tid < 32)
+  {
+    // node test of cell cx0 + tid: quadtree node origin away from the border
+    const int x = (cx0 + tid) * 4, y = cy * 4;
+    bool node = false;
+    if (tid < ncells && x > 0 && y > 0 && x < W - 1 && y < H - 1)
+    {
+      const int size = 1 << J.levels[(size_t)y * W + x];
+      node = x % size == 0 && y % size == 0;
+    }
+    const unsigned ballot = __ballot_sync(0xffffffffu, node);
+    if (node)
+    {
+      const int k = __popc(ballot & ((1u << tid) - 1u));
+      s_col[k] = tid;
+      const float3 dir = A::ray((float)x, (float)y, cam);
+      s_dir[0][k] = dir.x;
+      s_dir[1][k] = dir.y;
+      s_dir[2][k] = dir.z;
+      const uint8_t *r = J.ref + (size_t)(y - 1) * J.ref_pitch + (x - 1);
+#pragma unroll
+      for (int jj = 0; jj < 3; ++jj)
+#pragma unroll
+        for (int ii = 0; ii < 3; ++ii)
+          s_patch[3 * jj + ii][k] = __ldg(r + (size_t)jj * J.ref_pitch + ii);
+    }
+    if (tid == 0)
+      s_nodes = __popc(ballot);
+  }
+  __syncthreads();
+  const int n = s_nodes;
   const int pitch = J.slot_pitch;
   // (int)(u + 0.5) in [2, W-2) exactly when u in [1.5, W-2.5) (both bounds
   // are floats, the comparisons exact; NaN fails)
   const float ulo = 1.5f, uhi = (float)W - 2.5f, vhi = (float)H - 2.5f;
   const unsigned bias = 0u - kHalfBias * ((unsigned)pitch + 1u);
-  int sad = 0, nvalid = 0;
-  for (int f = 0; f < F; ++f)
+  // (node, hypothesis) pairs, node fastest: lanes of a warp hold
+  // neighbouring nodes, whose projections are neighbours in the slot images
+  if (n > 0)
   {
-    float T[12];
-    const float4 t0 = s_pose[3 * f], t1 = s_pose[3 * f + 1], t2 = s_pose[3 * f + 2];
-    T[0] = t0.x, T[1] = t0.y, T[2] = t0.z, T[3] = t0.w;
-    T[4] = t1.x, T[5] = t1.y, T[6] = t1.z, T[7] = t1.w;
-    T[8] = t2.x, T[9] = t2.y, T[10] = t2.z, T[11] = t2.w;
-    const float3 q = A::apply(T, p);
-    const float2 uv = A::project(q, cam);
-    if (uv.x >= ulo && uv.x < uhi && uv.y >= ulo && uv.y < vhi)
+    const int step_d = blockDim.x / n, step_k = blockDim.x - step_d * n;
+    int k = tid % n, d = tid / n;
+    for (; d < D; d += step_d)
     {
-      const uint8_t *m = s_img[f];
-      // The slot poses are validated as rigid on the host (|r00|+|r01| and
-      // |r10|+|r11| <= 1.5), so every patch coordinate + 0.5 lies in
-      // [0.5, W-0.5) x [0.5, H-0.5): no clamp needed.
-      float px[9], py[9];
-      patch_axis(uv.x, T[0], T[1], px);
-      patch_axis(uv.y, T[4], T[5], py);
-      unsigned s = 0;
-#pragma unroll
-      for (int k = 0; k < 9; ++k)
+      const float3 dir = make_float3(s_dir[0][k], s_dir[1][k], s_dir[2][k]);
+      const float3 p = A::scale(dir, s_depth[d]);
+      int sad = 0, nvalid = 0;
+      for (int f = 0; f < F; ++f)
       {
-        // offset = floor(py+0.5)*pitch + floor(px+0.5), in 32-bit wrap-around
-        // arithmetic (the true offset is below 2^31)
-        const unsigned hx = twice_round_bits(px[k]) >> 1;
-        const unsigned hy = twice_round_bits(py[k]) >> 1;
-        const unsigned off = hy * (unsigned)pitch + hx + bias;
-        s = __usad((unsigned)patch[k % 3][k / 3], (unsigned)__ldg(m + off), s);
+        float T[12];
+        const float4 t0 = s_pose[3 * f], t1 = s_pose[3 * f + 1], t2 = s_pose[3 * f + 2];
+        T[0] = t0.x, T[1] = t0.y, T[2] = t0.z, T[3] = t0.w;
+        T[4] = t1.x, T[5] = t1.y, T[6] = t1.z, T[7] = t1.w;
+        T[8] = t2.x, T[9] = t2.y, T[10] = t2.z, T[11] = t2.w;
+        const float3 q = A::apply(T, p);
+        const float2 uv = A::project(q, cam);
+        if (uv.x >= ulo && uv.x < uhi && uv.y >= ulo && uv.y < vhi)
+        {
+          const uint8_t *m = s_img[f];
+          // The slot poses are validated as rigid on the host (|r00|+|r01|
+          // and |r10|+|r11| <= 1.5), so every patch coordinate + 0.5 lies
+          // in [0.5, W-0.5) x [0.5, H-0.5): no clamp needed.
+          float px[9], py[9];
+          patch_axis(uv.x, T[0], T[1], px);
+          patch_axis(uv.y, T[4], T[5], py);
+          unsigned s = 0;
+#pragma unroll
+          for (int t = 0; t < 9; ++t)
+          {
+            // offset = floor(py+0.5)*pitch + floor(px+0.5), in 32-bit
+            // wrap-around arithmetic (the true offset is below 2^31)
+            const unsigned hx = twice_round_bits(px[t]) >> 1;
+            const unsigned hy = twice_round_bits(py[t]) >> 1;
+            const unsigned off = hy * (unsigned)pitch + hx + bias;
+            s = __usad((unsigned)s_patch[t][k], (unsigned)__ldg(m + off), s);
+          }
+          const int wgt = s_w[f];
+          sad += wgt * (int)s;
+          nvalid += wgt;
+        }
       }
-      const int wgt = s_w[f];
-      sad += wgt * (int)s;
-      nvalid += wgt;
+      const float c = nvalid > 0 ? A::sad_norm((float)sad, (float)nvalid) : 100.0f;
+      const int add_num = D; // writer count of the cell (see above)
+      s_out[s_col[k] * sd + d] = A::div(c, (float)add_num);
+      k += step_k;
+      if (k >= n)
+      {
+        k -= n;
+        ++d;
+      }
     }
   }
-  float c = nvalid > 0 ? A::sad_norm((float)sad, (float)nvalid) : 100.0f;
-  const int add_num = D; // writer count of the cell (see above)
-  *out = A::div(c, (float)add_num);
+  __syncthreads();
+  // the tile's cells are consecutive in the [cell][D] layout
+  float *out = J.lv[0].data + ((size_t)cy * J.cw + cx0) * D;
+  for (int i = tid; i < ncells * D; i += blockDim.x)
+  {
+    const int c = i / D;
+    out[i] = s_out[c * sd + (i - c * D)];
+  }
 }
 
 } // namespace
 
-void launch_cost(const Batch &B, int blocks, int arith, cudaStream_t s)
+int cost_blocks(int cw, int ch) { return ch * ((cw + kCostCells - 1) / kCostCells); }
+
+void launch_cost(const Batch &B, int blocks, int arith, int max_d, cudaStream_t s)
 {
+  const size_t sm = sizeof(float) * kCostCells * (max_d + 1);
   if (arith == QM_ARITH_IEEE)
-    k_cost<ArithIeee><<<blocks, kFlatThreads, 0, s>>>(B);
+    k_cost<ArithIeee><<<blocks, kFlatThreads, sm, s>>>(B);
   else
-    k_cost<ArithRef><<<blocks, kFlatThreads, 0, s>>>(B);
+    k_cost<ArithRef><<<blocks, kFlatThreads, sm, s>>>(B);
 }
 
 } // namespace qm
