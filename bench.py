@@ -381,11 +381,12 @@ def main():
     clocks = clk.summary()
 
     # ---- end-to-end: host frames in, host depth out, through the C-ABI
+    out_np = [t.numpy() for t in out_pinned]
+
     def e2e_step(j):
         i = WARM_FRAMES + (j % CYCLE_FRAMES)
         feed(i)
-        for s in range(S):
-            batch.get_depth(s, out=out_pinned[s].numpy())
+        batch.get_depths(outs=out_np)
 
     for j in range(args.warmup):
         e2e_step(j)

@@ -139,6 +139,11 @@ int qm_batch_add_frames(qm_batch *b, const uint8_t *const *imgs, const size_t *s
                         const float *T_curr_world, int *has_result);
 int qm_batch_get_depth(qm_batch *b, int stream, float *out, size_t stride);
 int qm_batch_get_debug(qm_batch *b, int stream, float *out, size_t stride);
+/* Fused depth of n streams in one call: streams[k] is written to outs[k]
+ * (row pitch strides[k] elements); the downloads are issued together and
+ * waited for once. */
+int qm_batch_get_depths(qm_batch *b, int n, const int *streams, float *const *outs,
+                        const size_t *strides);
 /* Re-runs the dense pipeline of every stream on the frames already resident
  * on the device (no host transfers); used to time the device path alone. */
 int qm_batch_run_resident(qm_batch *b);

@@ -74,6 +74,7 @@ _SIGS = {
     "qm_batch_add_frames": (_I, [_P, _P, _P, _P, _P]),
     "qm_batch_get_depth": (_I, [_P, _I, _P, _S]),
     "qm_batch_get_debug": (_I, [_P, _I, _P, _S]),
+    "qm_batch_get_depths": (_I, [_P, _I, _P, _P, _P]),
     "qm_batch_run_resident": (_I, [_P]),
     "qm_batch_device_depth": (_I, [_P, _I, ctypes.POINTER(_P)]),
     "qm_batch_set_graphs": (_I, [_P, _I]),

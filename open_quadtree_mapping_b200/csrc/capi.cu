@@ -363,6 +363,16 @@ int qm_batch_set_graphs(qm_batch *b, int enable)
   });
 }
 
+int qm_batch_get_depths(qm_batch *b, int n, const int *streams, float *const *outs,
+                        const size_t *strides)
+{
+  return guarded([&] {
+    require(b && n >= 0 && (n == 0 || (streams && outs && strides)), "bad argument");
+    std::lock_guard<std::mutex> lock(b->set->mutex());
+    b->set->get_depths(streams, n, outs, strides);
+  });
+}
+
 int qm_batch_set_group_bytes(qm_batch *b, size_t bytes)
 {
   return guarded([&] {

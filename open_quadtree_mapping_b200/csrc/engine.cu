@@ -63,9 +63,10 @@ std::vector<int> stage_blocks(const Shape &s, const JobLayout &lay, const qm_par
     b[st.pyr(l)] = cdiv((long)lay.lw[l] * lay.lh[l] * (D / 4), kFlatThreads);
   for (int l = 0; l < L; ++l)
     b[st.inherit(l)] = cdiv((long)lay.lw[l] * lay.lh[l] * (D / 4), kFlatThreads);
+  const int cpb = kCellWarps * bp_cells_per_warp(D); // BP cells per block
   for (int l = 0; l < L; ++l)
-    b[st.sweep(l)] = cdiv((long)((lay.lw[l] + 1) / 2) * lay.lh[l], kCellWarps);
-  b[st.extract()] = cdiv((long)lay.lw[0] * lay.lh[0], kCellWarps);
+    b[st.sweep(l)] = cdiv((long)((lay.lw[l] + 1) / 2) * lay.lh[l], cpb);
+  b[st.extract()] = cdiv((long)lay.lw[0] * lay.lh[0], cpb);
   b[st.row()] = cdiv(s.H, kRowWarps);
   b[st.col()] = cdiv(s.W, kColLines);
   b[st.ftrans()] = b[st.ffill()] = b[st.fupd()] = cdiv((long)s.W * s.H, kFlatThreads);

@@ -7,15 +7,19 @@
 // place; they only read messages of the other colour, so the update is a
 // Jacobi step inside the colour, exactly as the reference's launch.
 //
-// Warp-per-cell: lane l holds hypotheses l, l+32, l+64, ... of the cell.  The
-// four directions are computed from one load of the data cost and the four
+// Lane groups: a cell is handled by a group of LPC lanes (32 for 96 and 128
+// hypotheses, 16 for 48 and 64, 8 for 32), so a warp updates 32/LPC cells
+// at once; lane g of a group holds hypotheses g, g+LPC, g+2*LPC, ... (3 or
+// 4 register slots; every supported count is exactly LPC x slots).  The four
+// directions are computed from one load of the data cost and the four
 // incoming messages.  The normalising sum uses the reference's stride-halving
-// tree (bpextract.cu:293-300): strides >= 32 combine register slots, strides
-// 16..1 use __shfl_down, so lane 0 ends with the bit-identical sum.  The
-// argmin of the extraction uses the same tree with the reference's tie rule
-// (the right element wins only when strictly smaller, bpextract.cu:347-355).
-// Hypothesis counts that are not a power of two run the tree over the next
-// power of two with neutral padding (0 for sums, +inf for minima).
+// tree (bpextract.cu:293-300) over the next power of two P >= D with zero
+// padding: strides >= LPC combine register slots, strides < LPC run as an
+// xor butterfly inside the group, so lane 0 of the group ends with the
+// bit-identical sum (and, addition being commutative, so does every lane).
+// The argmin of the extraction uses the same tree with the reference's tie
+// rule (the right element wins only when strictly smaller,
+// bpextract.cu:347-355).
 //
 // Bytes per updated cell and half-sweep: 9*D*4 (data + 4 messages read, 4
 // messages written).
@@ -40,28 +44,33 @@ constexpr __host__ __device__ int pow2_ceil(int n)
 template <int D>
 struct HypLayout
 {
-  static constexpr int NV = (D + 31) / 32; // register slots per lane
-  static constexpr int P = pow2_ceil(D);   // tree width
+  static constexpr int P = pow2_ceil(D);              // tree width
+  static constexpr int LPC = P / 4 < 32 ? P / 4 : 32; // lanes per cell
+  static constexpr int NV = (D + LPC - 1) / LPC;      // register slots per lane
+  static constexpr int G = 32 / LPC;                  // cells per warp
+  static_assert(NV * LPC == D, "hypothesis count must fill the lane group");
 };
 
-// Stride-halving tree sum over D values held as v[k] = value(lane + 32k).
-// Strides >= 32 combine register slots; strides 16..1 run as an xor
-// butterfly.  Lane 0 performs exactly the reference's additions, and since
-// a + b == b + a bit for bit, every lane ends with lane 0's value, so no
-// broadcast is needed.
+// Stride-halving tree sum over the D values of a lane group, held as
+// v[k] = value(g + LPC*k).  Strides >= LPC combine register slots (the
+// padding beyond D is zero, so those additions are skipped); strides < LPC
+// run as an xor butterfly inside the group.  Lane 0 of the group performs
+// exactly the reference's additions, and since a + b == b + a bit for bit,
+// every lane of the group ends with lane 0's value.
 template <int D>
-__device__ __forceinline__ float tree_sum(float (&v)[HypLayout<D>::NV])
+__device__ __forceinline__ float tree_sum(const float (&v)[HypLayout<D>::NV])
 {
   constexpr int P = HypLayout<D>::P;
   constexpr int NV = HypLayout<D>::NV;
+  constexpr int LPC = HypLayout<D>::LPC;
   float a[NV];
 #pragma unroll
   for (int k = 0; k < NV; ++k)
     a[k] = v[k];
 #pragma unroll
-  for (int s = P / 2; s >= 32; s /= 2)
+  for (int s = P / 2; s >= LPC; s /= 2)
   {
-    const int t = s / 32;
+    const int t = s / LPC;
 #pragma unroll
     for (int k = 0; k < t; ++k)
       if (k + t < NV)
@@ -69,7 +78,7 @@ __device__ __forceinline__ float tree_sum(float (&v)[HypLayout<D>::NV])
   }
   float r = a[0];
 #pragma unroll
-  for (int o = (P / 2 < 16 ? P / 2 : 16); o > 0; o >>= 1)
+  for (int o = LPC / 2; o > 0; o >>= 1)
     r += __shfl_xor_sync(0xffffffffu, r, o);
   return r;
 }
@@ -88,24 +97,37 @@ __device__ __forceinline__ float warp_min_redux(float v)
   return __int_as_float(k ^ ((k >> 31) & 0x7fffffff));
 }
 
+// minimum over a lane group (exact, order-free)
+template <int LPC>
+__device__ __forceinline__ float group_min(float v)
+{
+  if (LPC == 32)
+    return warp_min_redux(v);
+#pragma unroll
+  for (int o = LPC / 2; o > 0; o >>= 1)
+    v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
 template <int D>
-__device__ __forceinline__ void tree_argmin(const float (&v)[HypLayout<D>::NV], int lane,
+__device__ __forceinline__ void tree_argmin(const float (&v)[HypLayout<D>::NV], int gl,
                                             float &best_v, int &best_i)
 {
   constexpr int P = HypLayout<D>::P;
   constexpr int NV = HypLayout<D>::NV;
+  constexpr int LPC = HypLayout<D>::LPC;
   float a[NV];
   int ai[NV];
 #pragma unroll
   for (int k = 0; k < NV; ++k)
   {
     a[k] = v[k];
-    ai[k] = lane + 32 * k;
+    ai[k] = gl + LPC * k;
   }
 #pragma unroll
-  for (int s = P / 2; s >= 32; s /= 2)
+  for (int s = P / 2; s >= LPC; s /= 2)
   {
-    const int t = s / 32;
+    const int t = s / LPC;
 #pragma unroll
     for (int k = 0; k < t; ++k)
       if (k + t < NV && a[k + t] < a[k])
@@ -117,10 +139,10 @@ __device__ __forceinline__ void tree_argmin(const float (&v)[HypLayout<D>::NV], 
   float r = a[0];
   int ri = ai[0];
 #pragma unroll
-  for (int o = (P / 2 < 16 ? P / 2 : 16); o > 0; o >>= 1)
+  for (int o = LPC / 2; o > 0; o >>= 1)
   {
-    const float ov = __shfl_down_sync(0xffffffffu, r, o);
-    const int oi = __shfl_down_sync(0xffffffffu, ri, o);
+    const float ov = __shfl_down_sync(0xffffffffu, r, o, LPC);
+    const int oi = __shfl_down_sync(0xffffffffu, ri, o, LPC);
     if (ov < r)
     {
       r = ov;
@@ -236,27 +258,38 @@ __global__ void __launch_bounds__(kFlatThreads)
 }
 
 // ------------------------------------------------------------- sweep
-// bp kernel (bpextract.cu:200-312), one warp per cell of the active colour.
+// bp kernel (bpextract.cu:200-312), one lane group per cell of the active
+// colour.  Groups whose cell is skipped or out of range still take part in
+// the warp's shuffles (full masks) with zero inputs and store nothing.
 template <int D, int ARITH>
-__global__ void __launch_bounds__(kCellWarps * 32)
+__global__ void __launch_bounds__(kCellWarps * 32, 7)
     k_bp_sweep(const __grid_constant__ Batch B, int level, int parity, int first, KParams kp)
 {
-  constexpr int NV = HypLayout<D>::NV;
+  using HL = HypLayout<D>;
+  constexpr int NV = HL::NV, LPC = HL::LPC, G = HL::G;
   int lb;
   const JobDesc &J = job_of(B, lb);
   if (J.D != D)
     return;
   const LevelDesc &L = J.lv[level];
   const int w = L.w, h = L.h, hw = (w + 1) / 2;
-  const int warp = lb * kCellWarps + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
-  if (warp >= hw * h)
+  const int lane = threadIdx.x & 31, gl = lane & (LPC - 1);
+  const int item0 = (lb * kCellWarps + (threadIdx.x >> 5)) * G;
+  if (item0 >= hw * h)
+    return; // the whole warp
+  const int item = item0 + lane / LPC;
+  int x = 0, y = 0;
+  bool act = item < hw * h;
+  if (act)
+  {
+    y = item / hw;
+    x = 2 * (item - y * hw) + ((y + parity) & 1); // item - y*hw == x / 2
+    act = x < w && !bp_skipped(J, level, x, y, kp.qt_max);
+  }
+  if (!__any_sync(0xffffffffu, act))
     return;
-  const int y = warp / hw, bx = warp - y * hw;
-  const int x = 2 * bx + ((y + parity) & 1); // bx == x / 2
-  if (x >= w || bp_skipped(J, level, x, y, kp.qt_max))
-    return;
-  const bool has_u = y > 0, has_d = y < h - 1, has_l = x > 0, has_r = x < w - 1;
+  const bool has_u = act && y > 0, has_d = act && y < h - 1;
+  const bool has_l = act && x > 0, has_r = act && x < w - 1;
   const size_t c = (size_t)y * w + x;
 
   // Incoming messages: the neighbours' own ones, or in the first half-sweep
@@ -285,20 +318,20 @@ __global__ void __launch_bounds__(kCellWarps * 32)
 #pragma unroll
   for (int k = 0; k < NV; ++k)
   {
-    const int d = lane + 32 * k;
-    const bool in = d < D;
-    dat[k] = in ? L.data[c * D + d] : 0.0f;
-    fu[k] = (in && ld && has_u) ? src_u[d] : 0.0f;
-    fd[k] = (in && ld && has_d) ? src_d[d] : 0.0f;
-    fl[k] = (in && ld && has_l) ? src_l[d] : 0.0f;
-    fr[k] = (in && ld && has_r) ? src_r[d] : 0.0f;
+    const int d = gl + LPC * k;
+    dat[k] = act ? L.data[c * D + d] : 0.0f;
+    fu[k] = (ld && has_u) ? src_u[d] : 0.0f;
+    fd[k] = (ld && has_d) ? src_d[d] : 0.0f;
+    fl[k] = (ld && has_l) ? src_l[d] : 0.0f;
+    fr[k] = (ld && has_r) ? src_r[d] : 0.0f;
   }
   const float P1 = kp.P1, P2 = kp.P2;
+  // h of every direction: the data term plus the three other incoming
+  // messages, in the reference's order (up, down, left, right skipped as
+  // named by the direction); computed up front so the raw inputs die early
+  float hall[4][NV];
 #pragma unroll
   for (int dir = 0; dir < 4; ++dir)
-  {
-    float hv[NV];
-    float lmin = FLT_MAX;
 #pragma unroll
     for (int k = 0; k < NV; ++k)
     {
@@ -311,79 +344,95 @@ __global__ void __launch_bounds__(kCellWarps * 32)
         v += fl[k];
       if (dir != kRight && has_r)
         v += fr[k];
-      const bool in = lane + 32 * k < D;
-      hv[k] = in ? v : FLT_MAX;
-      lmin = fminf(lmin, hv[k]);
+      hall[dir][k] = v;
     }
-    const float hmin = warp_min_redux(lmin);
+#pragma unroll
+  for (int dir = 0; dir < 4; ++dir)
+  {
+    const float(&hv)[NV] = hall[dir];
+    float lmin = FLT_MAX;
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+      lmin = fminf(lmin, hv[k]);
+    const float hmin = group_min<LPC>(lmin);
     float m[NV];
 #pragma unroll
     for (int k = 0; k < NV; ++k)
     {
-      const int d = lane + 32 * k;
-      // h(d-1): lane-1's slot k, or for lane 0 lane 31's slot k-1; h(d+1):
-      // lane+1's slot k, or for lane 31 lane 0's slot k+1.  One shuffle each,
-      // the source lane choosing which register it offers.
-      const float up_src = (lane == 31 && k > 0) ? hv[k > 0 ? k - 1 : 0] : hv[k];
-      const float dn_src = (lane == 0 && k + 1 < NV) ? hv[k + 1 < NV ? k + 1 : k] : hv[k];
-      const float prev = __shfl_sync(0xffffffffu, up_src, (lane + 31) & 31);
-      const float next = __shfl_sync(0xffffffffu, dn_src, (lane + 1) & 31);
+      const int d = gl + LPC * k;
+      // h(d-1): the previous lane's slot k, or for group lane 0 the group's
+      // last lane's slot k-1; h(d+1): the next lane's slot k, or for the last
+      // lane group lane 0's slot k+1.  One shuffle each, the source lane
+      // choosing which register it offers.
+      const float up_src = (gl == LPC - 1 && k > 0) ? hv[k > 0 ? k - 1 : 0] : hv[k];
+      const float dn_src = (gl == 0 && k + 1 < NV) ? hv[k + 1 < NV ? k + 1 : k] : hv[k];
+      const float prev = __shfl_sync(0xffffffffu, up_src, (gl + LPC - 1) & (LPC - 1), LPC);
+      const float next = __shfl_sync(0xffffffffu, dn_src, (gl + 1) & (LPC - 1), LPC);
       float mv = hv[k];
       if (d > 0)
         mv = fminf(mv, prev + P1);
       if (d < D - 1)
         mv = fminf(mv, next + P1);
-      mv = fminf(mv, hmin + P2);
-      m[k] = d < D ? mv : 0.0f;
+      m[k] = fminf(mv, hmin + P2);
     }
     const float sum = tree_sum<D>(m);
     const float mean = mean_of<D, ARITH>(sum);
-    float *out = L.msg[dir] + c * D;
-#pragma unroll
-    for (int k = 0; k < NV; ++k)
+    if (act)
     {
-      const int d = lane + 32 * k;
-      if (d < D)
-        out[d] = m[k] - mean;
+      float *out = L.msg[dir] + c * D;
+#pragma unroll
+      for (int k = 0; k < NV; ++k)
+        out[gl + LPC * k] = m[k] - mean;
     }
   }
 }
 
 // ------------------------------------------------------------- extract
-// depth_extract (bpextract.cu:314-372), one warp per level-0 cell.
+// depth_extract (bpextract.cu:314-372), one lane group per level-0 cell.
 template <int D, int ARITH>
 __global__ void __launch_bounds__(kCellWarps * 32)
     k_extract(const __grid_constant__ Batch B)
 {
-  constexpr int NV = HypLayout<D>::NV;
+  using HL = HypLayout<D>;
+  constexpr int NV = HL::NV, LPC = HL::LPC, G = HL::G;
   int lb;
   const JobDesc &J = job_of(B, lb);
   if (J.D != D)
     return;
   const LevelDesc &L = J.lv[0];
   const int w = L.w, h = L.h;
-  const int cell = lb * kCellWarps + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
-  if (cell >= w * h)
-    return;
-  const int x = cell % w, y = cell / w;
-  const int lvl = J.levels[(size_t)min(y * 4, J.H - 1) * J.W + min(x * 4, J.W - 1)];
-  const int size = 1 << lvl;
-  if ((x * 4) % size != 0 || (y * 4) % size != 0)
+  const int lane = threadIdx.x & 31, gl = lane & (LPC - 1);
+  const int cell0 = (lb * kCellWarps + (threadIdx.x >> 5)) * G;
+  if (cell0 >= w * h)
+    return; // the whole warp
+  const int cell = cell0 + lane / LPC;
+  bool act = cell < w * h;
+  int x = 0, y = 0;
+  if (act)
   {
-    if (lane == 0 && J.labels)
-      J.labels[cell] = -1;
-    return;
+    x = cell % w;
+    y = cell / w;
+    const int lvl = J.levels[(size_t)min(y * 4, J.H - 1) * J.W + min(x * 4, J.W - 1)];
+    const int size = 1 << lvl;
+    if ((x * 4) % size != 0 || (y * 4) % size != 0)
+    {
+      if (gl == 0 && J.labels)
+        J.labels[cell] = -1;
+      act = false;
+    }
   }
+  if (!__any_sync(0xffffffffu, act))
+    return;
   const size_t c = (size_t)cell;
   float b[NV];
 #pragma unroll
   for (int k = 0; k < NV; ++k)
   {
-    const int d = lane + 32 * k;
-    if (d < D)
+    const int d = gl + LPC * k;
+    float v = 0.0f;
+    if (act)
     {
-      float v = L.data[c * D + d];
+      v = L.data[c * D + d];
       if (x != 0)
         v += L.msg[kRight][(c - 1) * D + d];
       if (x != w - 1)
@@ -392,32 +441,28 @@ __global__ void __launch_bounds__(kCellWarps * 32)
         v += L.msg[kDown][(c - w) * D + d];
       if (y != h - 1)
         v += L.msg[kUp][(c + w) * D + d];
-      b[k] = v;
     }
-    else
-    {
-      b[k] = __int_as_float(0x7f800000); // +inf padding
-    }
+    b[k] = v;
   }
   float bmin;
   int best;
-  tree_argmin<D>(b, lane, bmin, best);
-  best = __shfl_sync(0xffffffffu, best, 0);
-  bmin = __shfl_sync(0xffffffffu, bmin, 0);
+  tree_argmin<D>(b, gl, bmin, best);
+  best = __shfl_sync(0xffffffffu, best, 0, LPC);
+  bmin = __shfl_sync(0xffffffffu, bmin, 0, LPC);
   // neighbours of the winner for the parabola
   const int ip = best > 0 ? best - 1 : 0, in_ = best < D - 1 ? best + 1 : D - 1;
   float pre = 0.0f, post = 0.0f;
 #pragma unroll
   for (int k = 0; k < NV; ++k)
   {
-    const float vp = __shfl_sync(0xffffffffu, b[k], ip & 31);
-    const float vn = __shfl_sync(0xffffffffu, b[k], in_ & 31);
-    if ((ip >> 5) == k)
+    const float vp = __shfl_sync(0xffffffffu, b[k], ip % LPC, LPC);
+    const float vn = __shfl_sync(0xffffffffu, b[k], in_ % LPC, LPC);
+    if (ip / LPC == k)
       pre = vp;
-    if ((in_ >> 5) == k)
+    if (in_ / LPC == k)
       post = vn;
   }
-  if (lane != 0)
+  if (gl != 0 || !act)
     return;
   float disparity = (float)best;
   if (best > 0 && best < D - 1)
@@ -474,6 +519,19 @@ void extract_d(const Batch &B, int blocks, int arith,
 } // namespace
 
 bool bp_supported_d(int d) { return d == 32 || d == 48 || d == 64 || d == 96 || d == 128; }
+
+int bp_cells_per_warp(int d)
+{
+  switch (d)
+  {
+  case 32: return HypLayout<32>::G;
+  case 48: return HypLayout<48>::G;
+  case 64: return HypLayout<64>::G;
+  case 96: return HypLayout<96>::G;
+  case 128: return HypLayout<128>::G;
+  default: return 1;
+  }
+}
 
 void launch_pyramid(const Batch &B, int blocks, int level,
                     cudaStream_t s)

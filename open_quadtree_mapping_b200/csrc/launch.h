@@ -54,7 +54,9 @@ void launch_fuse_transform(const Batch &B, int blocks, int arith, cudaStream_t s
 void launch_fuse_fill(const Batch &B, int blocks, cudaStream_t s);
 void launch_fuse_update(const Batch &B, int blocks, cudaStream_t s);
 
-// supported hypothesis-count classes of the warp-per-cell kernels
+// supported hypothesis-count classes of the BP kernels
 bool bp_supported_d(int d);
+// cells one warp of the BP sweep / extraction handles for d hypotheses
+int bp_cells_per_warp(int d);
 
 } // namespace qm

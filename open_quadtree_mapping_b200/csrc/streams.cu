@@ -119,7 +119,8 @@ StreamSet::StreamSet(int device, const qm_params &p, const std::vector<StreamDes
     State &s = st_[i];
     s.d = descs[i];
     const size_t frame = (size_t)s.d.W * s.d.H;
-    check(cudaMalloc((void **)&s.pool, frame * (kRing + 2)), "frame pool allocation");
+    // ring + income + spare frames, and the image of the last result
+    check(cudaMalloc((void **)&s.pool, frame * (kRing + 3)), "frame pool allocation");
     for (int k = kRing + 1; k >= 0; --k)
       s.free_slots.push_back(k);
     s.income_T = s.keyframe_T = s.fuse_T = s.T_world_ref = SE3f::identity();
@@ -159,9 +160,6 @@ StreamSet::Outcome StreamSet::begin_frame(int i, const uint8_t *img, size_t stri
   check(cudaMemcpy2DAsync(frame_ptr(s, s.income_slot), W, img, stride, W, H,
                           cudaMemcpyHostToDevice, eng_->stream()),
         "image upload");
-  s.income_host.resize((size_t)W * H);
-  for (int y = 0; y < H; ++y)
-    std::memcpy(s.income_host.data() + (size_t)y * W, img + (size_t)y * stride, W);
   s.income_T = SE3f::from(T);
   if (!s.initialized)
   {
@@ -195,6 +193,17 @@ StreamSet::Outcome StreamSet::begin_frame(int i, const uint8_t *img, size_t stri
   return kOutput;
 }
 
+// The image of the last result stays on the device (a copy into the pool's
+// last slot, ordered after the frame's upload on the engine stream) and is
+// only downloaded when asked for.
+void StreamSet::keep_reference(State &s)
+{
+  check(cudaMemcpyAsync(ref_ptr(s), frame_ptr(s, s.income_slot), (size_t)s.d.W * s.d.H,
+                        cudaMemcpyDeviceToDevice, eng_->stream()),
+        "reference image copy");
+  s.has_ref = true;
+}
+
 void StreamSet::end_frame(int i)
 {
   State &s = st_[i];
@@ -205,7 +214,7 @@ void StreamSet::end_frame(int i)
     const JobBuffers &b = eng_->buffers(i);
     check(cudaMemsetAsync(b.dense, 0, P * sizeof(float), eng_->stream()), "memset");
     check(cudaMemsetAsync(b.sparse, 0, P * sizeof(float), eng_->stream()), "memset");
-    s.ref_host = s.income_host;
+    keep_reference(s);
     s.T_world_ref = s.income_T.inv();
   }
   else if (s.outcome == kNoOutput || s.outcome == kOutput)
@@ -223,7 +232,7 @@ void StreamSet::end_frame(int i)
     if (s.outcome == kOutput)
     {
       s.fuse_T = s.income_T;
-      s.ref_host = s.income_host;
+      keep_reference(s);
       s.T_world_ref = s.income_T.inv();
     }
   }
@@ -307,13 +316,29 @@ void StreamSet::get_debug(int i, float *out, size_t stride)
         "debug download");
 }
 
+void StreamSet::get_depths(const int *streams, int n, float *const *outs, const size_t *strides)
+{
+  for (int k = 0; k < n; ++k)
+    if (streams[k] < 0 || streams[k] >= size() || !outs[k] || strides[k] < (size_t)st_[streams[k]].d.W)
+      throw CudaError{QM_ERR_INVALID_ARG, "bad stream index, output pointer or stride"};
+  for (int k = 0; k < n; ++k)
+  {
+    const State &s = st_[streams[k]];
+    check(cudaMemcpy2DAsync(outs[k], strides[k] * sizeof(float), eng_->buffers(streams[k]).dense,
+                            s.d.W * sizeof(float), s.d.W * sizeof(float), s.d.H,
+                            cudaMemcpyDeviceToHost, eng_->stream()),
+          "depth download");
+  }
+  check(cudaStreamSynchronize(eng_->stream()), "depth download");
+}
+
 void StreamSet::get_reference(int i, uint8_t *out, size_t stride)
 {
   const State &s = st_[i];
-  if (s.ref_host.empty())
+  if (!s.has_ref)
     throw CudaError{QM_ERR_STATE, "no result yet"};
-  for (int y = 0; y < s.d.H; ++y)
-    std::memcpy(out + (size_t)y * stride, s.ref_host.data() + (size_t)y * s.d.W, s.d.W);
+  check(cudaMemcpy2D(out, stride, ref_ptr(s), s.d.W, s.d.W, s.d.H, cudaMemcpyDeviceToHost),
+        "reference download");
 }
 
 void StreamSet::get_T_world_ref(int i, float *T) const

@@ -50,6 +50,8 @@ public:
   void get_depth(int i, float *out, size_t stride);
   void get_debug(int i, float *out, size_t stride);
   void get_reference(int i, uint8_t *out, size_t stride);
+  // fused depth of several streams: all downloads enqueued, one wait
+  void get_depths(const int *streams, int n, float *const *outs, const size_t *strides);
   void get_T_world_ref(int i, float *T) const;
   const StreamDesc &desc(int i) const { return st_[i].d; }
   const float *device_depth(int i) const { return eng_->buffers(i).dense; }
@@ -80,8 +82,7 @@ private:
     int frame_index = 0;
     bool initialized = false;
     Outcome outcome = kSkip;
-    std::vector<uint8_t> income_host; // copy of the frame being processed
-    std::vector<uint8_t> ref_host;    // image of the last result
+    bool has_ref = false; // the pool's last slot holds the last result's image
     SE3f T_world_ref;
   };
 
@@ -93,6 +94,8 @@ private:
   {
     return s.pool + (size_t)slot * s.d.W * s.d.H;
   }
+  uint8_t *ref_ptr(const State &s) const { return frame_ptr(s, QM_RING_CAPACITY + 2); }
+  void keep_reference(State &s);
 
   int device_;
   std::vector<State> st_;

@@ -178,6 +178,23 @@ class BatchDepthmap:
                                                  out.strides[0] // 4))
         return out
 
+    def get_depths(self, outs=None, streams=None) -> list:
+        """Fused depth of several streams (default: all) in one call; `outs`
+        are float32 (H, W) arrays with unit column stride (pinned memory
+        makes the downloads fastest)."""
+        streams = list(range(len(self.shapes))) if streams is None else list(streams)
+        if outs is None:
+            outs = [np.empty(self.shapes[i], np.float32) for i in streams]
+        n = len(streams)
+        for i, o in zip(streams, outs):
+            if o.dtype != np.float32 or o.shape != tuple(self.shapes[i]) or o.strides[1] != 4:
+                raise ValueError("output %d must be a float32 %s array" % (i, self.shapes[i]))
+        idx = (ctypes.c_int * n)(*streams)
+        ptrs = (ctypes.c_void_p * n)(*[o.ctypes.data for o in outs])
+        strides = (ctypes.c_size_t * n)(*[o.strides[0] // 4 for o in outs])
+        _lib.check(_lib.lib().qm_batch_get_depths(self._h, n, idx, ptrs, strides))
+        return outs
+
     def get_debug(self, i) -> np.ndarray:
         H, W = self.shapes[i]
         out = np.empty((H, W), np.float32)

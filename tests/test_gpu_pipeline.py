@@ -94,8 +94,10 @@ def test_batch_equals_plain_and_graph_equals_eager(gpu):
         hs = [singles[k].add_frames([imgs[k]], [poses[k]])[0] for k in range(3)]
         assert hb == he == hs
         if all(hb) and i > 0:
+            together = batch.get_depths()
             for k in range(3):
                 a = batch.get_depth(k)
+                assert np.array_equal(a, together[k])
                 assert np.array_equal(a, eager.get_depth(k))
                 assert np.array_equal(a, split.get_depth(k))
                 assert np.array_equal(a, whole.get_depth(k))
