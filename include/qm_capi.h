@@ -137,6 +137,22 @@ int qm_batch_destroy(qm_batch *b);
  * num_streams*12 floats, has_result: num_streams ints (out). */
 int qm_batch_add_frames(qm_batch *b, const uint8_t *const *imgs, const size_t *strides,
                         const float *T_curr_world, int *has_result);
+/* Pipelined form of qm_batch_add_frames: runs the frame policy of every
+ * stream (has_result is final on return), enqueues the image uploads, the
+ * dense pipeline and, for every stream i with a result and depth_outs[i] !=
+ * NULL, the download of its fused depth into depth_outs[i] (row pitch
+ * depth_strides[i] elements; NULL strides = dense rows), and returns
+ * without waiting.  Up to two steps are in flight, so the uploads of one
+ * step and the downloads of the previous one overlap the pipeline; host
+ * buffers should be pinned for the copies to be asynchronous.  imgs may be
+ * reused once the next qm_batch_submit or qm_batch_wait returns; depth_outs
+ * are complete once qm_batch_wait returns (every other batch call also
+ * waits first).  depth_outs may be NULL. */
+int qm_batch_submit(qm_batch *b, const uint8_t *const *imgs, const size_t *strides,
+                    const float *T_curr_world, int *has_result, float *const *depth_outs,
+                    const size_t *depth_strides);
+/* Waits for every submitted step. */
+int qm_batch_wait(qm_batch *b);
 int qm_batch_get_depth(qm_batch *b, int stream, float *out, size_t stride);
 int qm_batch_get_debug(qm_batch *b, int stream, float *out, size_t stride);
 /* Fused depth of n streams in one call: streams[k] is written to outs[k]

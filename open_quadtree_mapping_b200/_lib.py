@@ -73,6 +73,8 @@ _SIGS = {
     "qm_batch_destroy": (_I, [_P]),
     "qm_batch_add_frames": (_I, [_P, _P, _P, _P, _P]),
     "qm_batch_get_depth": (_I, [_P, _I, _P, _S]),
+    "qm_batch_submit": (_I, [_P, _P, _P, _P, _P, _P, _P]),
+    "qm_batch_wait": (_I, [_P]),
     "qm_batch_get_debug": (_I, [_P, _I, _P, _S]),
     "qm_batch_get_depths": (_I, [_P, _I, _P, _P, _P]),
     "qm_batch_run_resident": (_I, [_P]),

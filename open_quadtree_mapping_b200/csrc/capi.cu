@@ -318,6 +318,26 @@ int qm_batch_add_frames(qm_batch *b, const uint8_t *const *imgs, const size_t *s
   });
 }
 
+int qm_batch_submit(qm_batch *b, const uint8_t *const *imgs, const size_t *strides,
+                    const float *T_curr_world, int *has_result, float *const *depth_outs,
+                    const size_t *depth_strides)
+{
+  return guarded([&] {
+    require(b && imgs && strides && T_curr_world && has_result, "NULL argument");
+    std::lock_guard<std::mutex> lock(b->set->mutex());
+    b->set->submit(imgs, strides, T_curr_world, has_result, depth_outs, depth_strides);
+  });
+}
+
+int qm_batch_wait(qm_batch *b)
+{
+  return guarded([&] {
+    require(b != nullptr, "NULL handle");
+    std::lock_guard<std::mutex> lock(b->set->mutex());
+    b->set->wait();
+  });
+}
+
 int qm_batch_get_depth(qm_batch *b, int stream, float *out, size_t stride)
 {
   return guarded([&] {
@@ -351,6 +371,8 @@ int qm_batch_device_depth(qm_batch *b, int stream, const float **dev_ptr)
 {
   return guarded([&] {
     require(b && dev_ptr && stream >= 0 && stream < b->set->size(), "bad argument");
+    std::lock_guard<std::mutex> lock(b->set->mutex());
+    b->set->wait();
     *dev_ptr = b->set->device_depth(stream);
   });
 }

@@ -354,7 +354,8 @@ JobLayout JobLayout::make(const Shape &s, int nlev)
   }
   L.off_labels = take((size_t)(s.W / 4) * (s.H / 4) * sizeof(int32_t));
   L.off_sparse = take(P * sizeof(float));
-  L.off_dense = take(P * sizeof(float));
+  L.off_dense[0] = take(P * sizeof(float));
+  L.off_dense[1] = take(P * sizeof(float));
   L.off_rowres = take(P * sizeof(float2));
   L.off_seeds[0] = take(P * sizeof(float4));
   L.off_seeds[1] = take(P * sizeof(float4));
@@ -392,7 +393,7 @@ JobDesc make_job_desc(const Shape &s, const qm_params &p, const JobBuffers &b, i
   }
   J.labels = b.labels;
   J.sparse = b.sparse;
-  J.dense = b.dense;
+  J.dense = b.dense[0];
   J.rowres = b.rowres;
   J.seeds_in = b.seeds[seeds_cur];
   J.seeds_out = b.seeds[seeds_cur ^ 1];
@@ -408,12 +409,13 @@ struct Plan
   std::vector<int> active;
   int *d_prefix = nullptr;
   StageTable table;
-  size_t group_bytes = 0; // the job grouping the graph was captured with
-  cudaGraphExec_t exec = nullptr;
+  size_t group_bytes = 0;              // the job grouping the graphs were captured with
+  cudaGraphExec_t exec[2] = {nullptr, nullptr}; // by step parity
   ~Plan()
   {
-    if (exec)
-      cudaGraphExecDestroy(exec);
+    for (auto e : exec)
+      if (e)
+        cudaGraphExecDestroy(e);
     if (d_prefix)
       cudaFree(d_prefix);
   }
@@ -469,7 +471,8 @@ Engine::Engine(int device, const qm_params &p, const std::vector<Shape> &shapes)
     }
     B.labels = (int32_t *)(b0 + L.off_labels);
     B.sparse = (float *)(b0 + L.off_sparse);
-    B.dense = (float *)(b0 + L.off_dense);
+    B.dense[0] = (float *)(b0 + L.off_dense[0]);
+    B.dense[1] = (float *)(b0 + L.off_dense[1]);
     B.rowres = (float2 *)(b0 + L.off_rowres);
     B.seeds[0] = (float4 *)(b0 + L.off_seeds[0]);
     B.seeds[1] = (float4 *)(b0 + L.off_seeds[1]);
@@ -480,7 +483,8 @@ Engine::Engine(int device, const qm_params &p, const std::vector<Shape> &shapes)
     check(cudaMemsetAsync(B.seeds[1], 0, P * sizeof(float4) * 1, stream_), "memset");
     check(cudaMemsetAsync(B.zkey, 0xff, P * sizeof(unsigned long long), stream_), "memset");
     check(cudaMemsetAsync(B.sparse, 0, P * sizeof(float), stream_), "memset");
-    check(cudaMemsetAsync(B.dense, 0, P * sizeof(float), stream_), "memset");
+    check(cudaMemsetAsync(B.dense[0], 0, P * sizeof(float), stream_), "memset");
+    check(cudaMemsetAsync(B.dense[1], 0, P * sizeof(float), stream_), "memset");
     check(cudaMemsetAsync(B.table, 0, P * sizeof(int32_t), stream_), "memset");
   }
   slot_base_.resize(n);
@@ -489,15 +493,22 @@ Engine::Engine(int device, const qm_params &p, const std::vector<Shape> &shapes)
     slot_base_[j] = total_slots_;
     total_slots_ += shapes[j].F;
   }
-  check(cudaHostAlloc((void **)&h_slot_ptr_, sizeof(void *) * total_slots_, cudaHostAllocDefault),
-        "pinned allocation");
-  check(cudaHostAlloc((void **)&h_slot_T_, sizeof(float) * 12 * total_slots_, cudaHostAllocDefault),
-        "pinned allocation");
-  check(cudaHostAlloc((void **)&h_slot_w_, sizeof(int) * total_slots_, cudaHostAllocDefault),
-        "pinned allocation");
-  std::memset(h_slot_ptr_, 0, sizeof(void *) * total_slots_);
-  std::memset(h_slot_T_, 0, sizeof(float) * 12 * total_slots_);
-  std::memset(h_slot_w_, 0, sizeof(int) * total_slots_);
+  for (int q = 0; q < 2; ++q)
+  {
+    check(cudaHostAlloc((void **)&h_slot_ptr_[q], sizeof(void *) * total_slots_,
+                        cudaHostAllocDefault),
+          "pinned allocation");
+    check(cudaHostAlloc((void **)&h_slot_T_[q], sizeof(float) * 12 * total_slots_,
+                        cudaHostAllocDefault),
+          "pinned allocation");
+    check(cudaHostAlloc((void **)&h_slot_w_[q], sizeof(int) * total_slots_, cudaHostAllocDefault),
+          "pinned allocation");
+    std::memset(h_slot_ptr_[q], 0, sizeof(void *) * total_slots_);
+    std::memset(h_slot_T_[q], 0, sizeof(float) * 12 * total_slots_);
+    std::memset(h_slot_w_[q], 0, sizeof(int) * total_slots_);
+    check(cudaHostAlloc((void **)&h_run_[q], sizeof(JobDesc) * n, cudaHostAllocDefault),
+          "pinned allocation");
+  }
   check(cudaMalloc((void **)&d_slot_ptr_, sizeof(void *) * total_slots_), "device allocation");
   check(cudaMalloc((void **)&d_slot_T_, sizeof(float) * 12 * total_slots_), "device allocation");
   check(cudaMalloc((void **)&d_slot_w_, sizeof(int) * total_slots_), "device allocation");
@@ -507,8 +518,6 @@ Engine::Engine(int device, const qm_params &p, const std::vector<Shape> &shapes)
     master_[j] = make_job_desc(shapes[j], p, bufs_[j], 0);
     master_[j].slot_base = slot_base_[j];
   }
-  check(cudaHostAlloc((void **)&h_run_, sizeof(JobDesc) * n, cudaHostAllocDefault),
-        "pinned allocation");
   check(cudaMalloc((void **)&d_run_, sizeof(JobDesc) * n), "device allocation");
   check(cudaStreamSynchronize(stream_), "engine init");
 }
@@ -529,14 +538,17 @@ Engine::~Engine()
     cudaFree(d_slot_w_);
   if (d_run_)
     cudaFree(d_run_);
-  if (h_slot_ptr_)
-    cudaFreeHost(h_slot_ptr_);
-  if (h_slot_T_)
-    cudaFreeHost(h_slot_T_);
-  if (h_slot_w_)
-    cudaFreeHost(h_slot_w_);
-  if (h_run_)
-    cudaFreeHost(h_run_);
+  for (int q = 0; q < 2; ++q)
+  {
+    if (h_slot_ptr_[q])
+      cudaFreeHost(h_slot_ptr_[q]);
+    if (h_slot_T_[q])
+      cudaFreeHost(h_slot_T_[q]);
+    if (h_slot_w_[q])
+      cudaFreeHost(h_slot_w_[q]);
+    if (h_run_[q])
+      cudaFreeHost(h_run_[q]);
+  }
   if (ev0_)
     cudaEventDestroy(ev0_);
   if (ev1_)
@@ -553,8 +565,9 @@ void Engine::set_inputs(int j, const uint8_t *ref, int ref_pitch, const uint8_t 
   J.ref_pitch = ref_pitch;
   J.slot_pitch = slot_pitch;
   const int b = slot_base_[j];
-  J.F = dedupe_slots(shapes_[j].F, slots, T_slot_ref, h_slot_ptr_ + b, h_slot_T_ + 12 * b,
-                     h_slot_w_ + b);
+  const int q = parity_;
+  J.F = dedupe_slots(shapes_[j].F, slots, T_slot_ref, h_slot_ptr_[q] + b, h_slot_T_[q] + 12 * b,
+                     h_slot_w_[q] + b);
   if (T_fuse)
     std::memcpy(J.Tf, T_fuse, 12 * sizeof(float));
 }
@@ -574,11 +587,13 @@ Plan &Engine::plan_for(const std::vector<int> &active)
   if (it != plans_.end())
   {
     Plan &pl = *it->second;
-    if (pl.exec && pl.group_bytes != group_bytes_)
-    {
-      cudaGraphExecDestroy(pl.exec);
-      pl.exec = nullptr;
-    }
+    if (pl.group_bytes != group_bytes_)
+      for (auto &e : pl.exec)
+        if (e)
+        {
+          cudaGraphExecDestroy(e);
+          e = nullptr;
+        }
     return pl;
   }
   auto pl = std::make_unique<Plan>();
@@ -620,21 +635,23 @@ void Engine::pack(const std::vector<int> &active)
     JobDesc J = master_[j];
     J.seeds_in = bufs_[j].seeds[seeds_cur_[j]];
     J.seeds_out = bufs_[j].seeds[seeds_cur_[j] ^ 1];
-    h_run_[i] = J;
+    J.dense = bufs_[j].dense[parity_];
+    h_run_[parity_][i] = J;
   }
 }
 
 Batch Engine::upload(int n, cudaStream_t s)
 {
-  check(cudaMemcpyAsync(d_run_, h_run_, sizeof(JobDesc) * n, cudaMemcpyHostToDevice, s),
+  const int q = parity_;
+  check(cudaMemcpyAsync(d_run_, h_run_[q], sizeof(JobDesc) * n, cudaMemcpyHostToDevice, s),
         "descriptor upload");
-  check(cudaMemcpyAsync(d_slot_ptr_, h_slot_ptr_, sizeof(void *) * total_slots_,
+  check(cudaMemcpyAsync(d_slot_ptr_, h_slot_ptr_[q], sizeof(void *) * total_slots_,
                         cudaMemcpyHostToDevice, s),
         "slot upload");
-  check(cudaMemcpyAsync(d_slot_T_, h_slot_T_, sizeof(float) * 12 * total_slots_,
+  check(cudaMemcpyAsync(d_slot_T_, h_slot_T_[q], sizeof(float) * 12 * total_slots_,
                         cudaMemcpyHostToDevice, s),
         "slot upload");
-  check(cudaMemcpyAsync(d_slot_w_, h_slot_w_, sizeof(int) * total_slots_,
+  check(cudaMemcpyAsync(d_slot_w_, h_slot_w_[q], sizeof(int) * total_slots_,
                         cudaMemcpyHostToDevice, s),
         "slot upload");
   Batch B;
@@ -657,6 +674,12 @@ int Engine::enqueue(Plan &pl, cudaStream_t s)
 
 void Engine::run(const std::vector<int> &active)
 {
+  launch(active);
+  check(cudaStreamSynchronize(stream_), "pipeline run");
+}
+
+void Engine::launch(const std::vector<int> &active)
+{
   if (active.empty())
     return;
   check(cudaSetDevice(device_), "cudaSetDevice");
@@ -664,7 +687,10 @@ void Engine::run(const std::vector<int> &active)
   pack(active);
   if (graphs_)
   {
-    if (!pl.exec)
+    // one graph per parity: its memcpy nodes read that parity's pinned
+    // descriptor and slot tables
+    cudaGraphExec_t &exec = pl.exec[parity_];
+    if (!exec)
     {
       cudaGraph_t g = nullptr;
       check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "graph capture");
@@ -681,13 +707,13 @@ void Engine::run(const std::vector<int> &active)
         throw;
       }
       check(cudaStreamEndCapture(stream_, &g), "graph capture");
-      const cudaError_t e = cudaGraphInstantiate(&pl.exec, g, 0);
+      const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
       cudaGraphDestroy(g);
       check(e, "graph instantiate");
       last_launches_ = nl;
     }
     check(cudaEventRecord(ev0_, stream_), "event");
-    check(cudaGraphLaunch(pl.exec, stream_), "graph launch");
+    check(cudaGraphLaunch(exec, stream_), "graph launch");
     check(cudaEventRecord(ev1_, stream_), "event");
   }
   else
@@ -696,7 +722,6 @@ void Engine::run(const std::vector<int> &active)
     last_launches_ = enqueue(pl, stream_);
     check(cudaEventRecord(ev1_, stream_), "event");
   }
-  check(cudaStreamSynchronize(stream_), "pipeline run");
   for (int j : active)
     seeds_cur_[j] ^= 1;
 }

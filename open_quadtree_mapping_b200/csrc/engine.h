@@ -78,7 +78,8 @@ struct JobBuffers
   int lw[kMaxLevels] = {}, lh[kMaxLevels] = {};
   int32_t *labels = nullptr;
   float *sparse = nullptr;
-  float *dense = nullptr;
+  float *dense[2] = {}; // by step parity (a step's result can be read
+                        // back while the next step runs)
   float2 *rowres = nullptr;
   float4 *seeds[2] = {};
   unsigned long long *zkey = nullptr;
@@ -90,7 +91,7 @@ struct JobLayout
 {
   size_t bytes = 0;
   size_t off_levels, off_data[kMaxLevels], off_msg[kMaxLevels][4], off_labels, off_sparse,
-      off_dense, off_rowres, off_seeds[2], off_zkey, off_table;
+      off_dense[2], off_rowres, off_seeds[2], off_zkey, off_table;
   int lw[kMaxLevels], lh[kMaxLevels];
   static JobLayout make(const Shape &s, int nlev);
 };
@@ -135,6 +136,14 @@ public:
   cudaStream_t stream() const { return stream_; }
   int device() const { return device_; }
 
+  // Step parity: selects the output buffer and the pinned descriptor and
+  // slot tables that set_inputs / launch use, so that the host can prepare
+  // step t+1 while step t (the other parity) is still in flight.
+  void set_parity(int p) { parity_ = p & 1; }
+  int parity() const { return parity_; }
+  // fused depth buffer of job j for the current parity
+  float *dense(int j) const { return bufs_[j].dense[parity_]; }
+
   // Inputs of job j for the next run.  Device pointers; T_slot_ref is
   // F*12 floats (host), T_fuse 12 floats T_income<-lastfuse (host).
   void set_inputs(int j, const uint8_t *ref, int ref_pitch, const uint8_t *const *slots,
@@ -143,8 +152,10 @@ public:
   float4 *seeds(int j) const { return bufs_[j].seeds[seeds_cur_[j]]; }
   void reset_seeds(int j);
 
-  // Runs the pipeline for `active` job indices and waits for it.  Throws
-  // CudaError.  Graph capture is used when `graphs` is set.
+  // Enqueues the pipeline for `active` job indices on stream() without
+  // waiting.  Throws CudaError.  Graph capture is used when `graphs` is set.
+  void launch(const std::vector<int> &active);
+  // launch() and wait for it
   void run(const std::vector<int> &active);
   void set_graphs(bool on) { graphs_ = on; }
   // L2 budget of a BP job range (0: every level over all jobs at once)
@@ -176,19 +187,20 @@ private:
   // slot tables (all jobs), pinned host + device
   std::vector<int> slot_base_;
   int total_slots_ = 0;
-  const uint8_t **h_slot_ptr_ = nullptr;
-  float *h_slot_T_ = nullptr;
-  int *h_slot_w_ = nullptr;
+  const uint8_t **h_slot_ptr_[2] = {};
+  float *h_slot_T_[2] = {};
+  int *h_slot_w_[2] = {};
   const uint8_t **d_slot_ptr_ = nullptr;
   float *d_slot_T_ = nullptr;
   int *d_slot_w_ = nullptr;
   // job descriptors: host master copy and the packed run arrays
   std::vector<JobDesc> master_;
-  JobDesc *h_run_ = nullptr;
+  JobDesc *h_run_[2] = {};
   JobDesc *d_run_ = nullptr;
   cudaStream_t stream_ = nullptr;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
   bool graphs_ = true;
+  int parity_ = 0;
   size_t group_bytes_ = kDefaultGroupBytes;
   int last_launches_ = 0;
   std::map<std::vector<int>, std::unique_ptr<Plan>> plans_;

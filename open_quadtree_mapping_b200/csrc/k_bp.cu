@@ -101,12 +101,15 @@ __device__ __forceinline__ float warp_min_redux(float v)
 template <int LPC>
 __device__ __forceinline__ float group_min(float v)
 {
-  if (LPC == 32)
+  if constexpr (LPC == 32)
     return warp_min_redux(v);
+  else
+  {
 #pragma unroll
-  for (int o = LPC / 2; o > 0; o >>= 1)
-    v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
-  return v;
+    for (int o = LPC / 2; o > 0; o >>= 1)
+      v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+  }
 }
 
 template <int D>

@@ -287,7 +287,7 @@ __global__ void __launch_bounds__(kColLines * 32)
   int lb;
   const JobDesc &J = job_of(B, lb);
   const int W = J.W, H = J.H;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
   const int x0 = lb * kColLines;
   const int n = H / 8 * 8;
   const int per_line = kArrays * line_floats(max_n);

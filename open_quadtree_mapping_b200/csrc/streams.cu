@@ -113,6 +113,14 @@ StreamSet::StreamSet(int device, const qm_params &p, const std::vector<StreamDes
     shapes.push_back(Shape{d.W, d.H, d.D, d.F, d.cam});
   }
   eng_ = std::make_unique<Engine>(device, p, shapes);
+  check(cudaStreamCreateWithFlags(&up_, cudaStreamNonBlocking), "cudaStreamCreate");
+  check(cudaStreamCreateWithFlags(&down_, cudaStreamNonBlocking), "cudaStreamCreate");
+  for (int q = 0; q < 2; ++q)
+  {
+    check(cudaEventCreateWithFlags(&ev_up_[q], cudaEventDisableTiming), "cudaEventCreate");
+    check(cudaEventCreateWithFlags(&ev_comp_[q], cudaEventDisableTiming), "cudaEventCreate");
+    check(cudaEventCreateWithFlags(&ev_done_[q], cudaEventDisableTiming), "cudaEventCreate");
+  }
   st_.resize(descs.size());
   for (size_t i = 0; i < descs.size(); ++i)
   {
@@ -130,6 +138,24 @@ StreamSet::StreamSet(int device, const qm_params &p, const std::vector<StreamDes
 StreamSet::~StreamSet()
 {
   cudaSetDevice(device_);
+  if (up_)
+    cudaStreamSynchronize(up_);
+  if (down_)
+    cudaStreamSynchronize(down_);
+  cudaStreamSynchronize(eng_->stream());
+  for (int q = 0; q < 2; ++q)
+  {
+    if (ev_up_[q])
+      cudaEventDestroy(ev_up_[q]);
+    if (ev_comp_[q])
+      cudaEventDestroy(ev_comp_[q]);
+    if (ev_done_[q])
+      cudaEventDestroy(ev_done_[q]);
+  }
+  if (up_)
+    cudaStreamDestroy(up_);
+  if (down_)
+    cudaStreamDestroy(down_);
   for (auto &s : st_)
     if (s.pool)
       cudaFree(s.pool);
@@ -157,9 +183,16 @@ StreamSet::Outcome StreamSet::begin_frame(int i, const uint8_t *img, size_t stri
   s.frame_index++;
   s.income_slot = s.free_slots.back();
   s.free_slots.pop_back();
-  check(cudaMemcpy2DAsync(frame_ptr(s, s.income_slot), W, img, stride, W, H,
-                          cudaMemcpyHostToDevice, eng_->stream()),
-        "image upload");
+  // a dense image goes up as one linear copy (row-by-row 2D copies of short
+  // rows are much slower on the copy engines)
+  if (stride == (size_t)W)
+    check(cudaMemcpyAsync(frame_ptr(s, s.income_slot), img, (size_t)W * H,
+                          cudaMemcpyHostToDevice, up_),
+          "image upload");
+  else
+    check(cudaMemcpy2DAsync(frame_ptr(s, s.income_slot), W, img, stride, W, H,
+                            cudaMemcpyHostToDevice, up_),
+          "image upload");
   s.income_T = SE3f::from(T);
   if (!s.initialized)
   {
@@ -204,7 +237,7 @@ void StreamSet::keep_reference(State &s)
   s.has_ref = true;
 }
 
-void StreamSet::end_frame(int i)
+void StreamSet::end_frame(int i, int parity)
 {
   State &s = st_[i];
   const size_t P = (size_t)s.d.W * s.d.H;
@@ -212,7 +245,7 @@ void StreamSet::end_frame(int i)
   if (s.outcome == kFirst)
   {
     const JobBuffers &b = eng_->buffers(i);
-    check(cudaMemsetAsync(b.dense, 0, P * sizeof(float), eng_->stream()), "memset");
+    check(cudaMemsetAsync(eng_->dense(i), 0, P * sizeof(float), eng_->stream()), "memset");
     check(cudaMemsetAsync(b.sparse, 0, P * sizeof(float), eng_->stream()), "memset");
     keep_reference(s);
     s.T_world_ref = s.income_T.inv();
@@ -225,7 +258,7 @@ void StreamSet::end_frame(int i)
       keep_income = true;
       if ((int)s.ring.size() > kRing)
       {
-        s.free_slots.push_back(s.ring.back().slot);
+        pending_[parity].push_back({i, s.ring.back().slot});
         s.ring.pop_back();
       }
     }
@@ -236,47 +269,120 @@ void StreamSet::end_frame(int i)
       s.T_world_ref = s.income_T.inv();
     }
   }
+  // a freed slot may still be read by this step's pipeline: it becomes free
+  // again once the step has retired
   if (!keep_income)
-    s.free_slots.push_back(s.income_slot);
+    pending_[parity].push_back({i, s.income_slot});
   s.income_slot = -1;
+}
+
+void StreamSet::retire(int p)
+{
+  if (!inflight_[p])
+    return;
+  check(cudaEventSynchronize(ev_done_[p]), "step");
+  for (const auto &f : pending_[p])
+    st_[f.first].free_slots.push_back(f.second);
+  pending_[p].clear();
+  inflight_[p] = false;
+}
+
+void StreamSet::wait()
+{
+  // the older step first, so slots return in the order they were freed
+  const int p = (int)(step_ & 1);
+  retire(p);
+  retire(p ^ 1);
+}
+
+void StreamSet::step(const std::vector<int> &which, const uint8_t *const *imgs,
+                     const size_t *strides, const float *T_curr_world, int *has_result,
+                     float *const *depth_outs, const size_t *depth_strides)
+{
+  check(cudaSetDevice(device_), "cudaSetDevice");
+  const int p = (int)(step_ & 1);
+  // step t-2 (same parity) must be done: its output buffer, pinned tables
+  // and freed slots are reused now; step t-1's uploads must be done so that
+  // the caller may reuse its image buffers
+  retire(p);
+  if (inflight_[p ^ 1])
+    check(cudaEventSynchronize(ev_up_[p ^ 1]), "upload");
+  eng_->set_parity(p);
+  std::vector<int> active;
+  for (size_t k = 0; k < which.size(); ++k)
+  {
+    const int i = which[k];
+    st_[i].outcome = begin_frame(i, imgs[k], strides[k], T_curr_world + 12 * k);
+    if (st_[i].outcome == kOutput)
+      active.push_back(i);
+  }
+  check(cudaEventRecord(ev_up_[p], up_), "event");
+  check(cudaStreamWaitEvent(eng_->stream(), ev_up_[p], 0), "event wait");
+  if (!active.empty())
+  {
+    eng_->launch(active);
+    last_active_ = active;
+  }
+  for (size_t k = 0; k < which.size(); ++k)
+  {
+    end_frame(which[k], p);
+    const Outcome o = st_[which[k]].outcome;
+    has_result[k] = (o == kFirst || o == kOutput) ? 1 : 0;
+    if (has_result[k])
+      st_[which[k]].out_parity = p;
+  }
+  check(cudaEventRecord(ev_comp_[p], eng_->stream()), "event");
+  check(cudaStreamWaitEvent(down_, ev_comp_[p], 0), "event wait");
+  if (depth_outs)
+    for (size_t k = 0; k < which.size(); ++k)
+    {
+      if (!has_result[k] || !depth_outs[k])
+        continue;
+      const State &s = st_[which[k]];
+      const float *src = eng_->dense(which[k]);
+      const size_t stride = depth_strides ? depth_strides[k] : (size_t)s.d.W;
+      if (stride == (size_t)s.d.W)
+        check(cudaMemcpyAsync(depth_outs[k], src, sizeof(float) * s.d.W * s.d.H,
+                              cudaMemcpyDeviceToHost, down_),
+              "depth download");
+      else
+        check(cudaMemcpy2DAsync(depth_outs[k], stride * sizeof(float), src,
+                                s.d.W * sizeof(float), s.d.W * sizeof(float), s.d.H,
+                                cudaMemcpyDeviceToHost, down_),
+              "depth download");
+    }
+  check(cudaEventRecord(ev_done_[p], down_), "event");
+  inflight_[p] = true;
+  ++step_;
+}
+
+void StreamSet::submit(const uint8_t *const *imgs, const size_t *strides,
+                       const float *T_curr_world, int *has_result, float *const *depth_outs,
+                       const size_t *depth_strides)
+{
+  if (depth_outs)
+    for (int i = 0; i < size(); ++i)
+      if (depth_outs[i] && depth_strides && depth_strides[i] < (size_t)st_[i].d.W)
+        throw CudaError{QM_ERR_INVALID_ARG, "depth stride smaller than the width"};
+  std::vector<int> all(size());
+  for (int i = 0; i < size(); ++i)
+    all[i] = i;
+  step(all, imgs, strides, T_curr_world, has_result, depth_outs, depth_strides);
 }
 
 void StreamSet::add_frames(const uint8_t *const *imgs, const size_t *strides,
                            const float *T_curr_world, int *has_result)
 {
-  check(cudaSetDevice(device_), "cudaSetDevice");
-  std::vector<int> active;
-  for (int i = 0; i < size(); ++i)
-  {
-    st_[i].outcome = begin_frame(i, imgs[i], strides[i], T_curr_world + 12 * i);
-    if (st_[i].outcome == kOutput)
-      active.push_back(i);
-  }
-  if (!active.empty())
-  {
-    eng_->run(active);
-    last_active_ = active;
-  }
-  for (int i = 0; i < size(); ++i)
-  {
-    end_frame(i);
-    has_result[i] = (st_[i].outcome == kFirst || st_[i].outcome == kOutput) ? 1 : 0;
-  }
-  check(cudaStreamSynchronize(eng_->stream()), "frame");
+  submit(imgs, strides, T_curr_world, has_result, nullptr, nullptr);
+  wait();
 }
 
 int StreamSet::add_frame(int i, const uint8_t *img, size_t stride, const float *T_curr_world)
 {
-  check(cudaSetDevice(device_), "cudaSetDevice");
-  st_[i].outcome = begin_frame(i, img, stride, T_curr_world);
-  if (st_[i].outcome == kOutput)
-  {
-    eng_->run({i});
-    last_active_ = {i};
-  }
-  end_frame(i);
-  check(cudaStreamSynchronize(eng_->stream()), "frame");
-  return (st_[i].outcome == kFirst || st_[i].outcome == kOutput) ? 1 : 0;
+  int has = 0;
+  step({i}, &img, &stride, T_curr_world, &has, nullptr, nullptr);
+  wait();
+  return has;
 }
 
 void StreamSet::run_resident()
@@ -288,7 +394,10 @@ void StreamSet::run_resident()
     all.push_back(i);
   if (last_active_ != all)
     throw CudaError{QM_ERR_STATE, "every stream must have produced a depth map once"};
+  wait();
   eng_->run(all);
+  for (auto &s : st_)
+    s.out_parity = eng_->parity();
 }
 
 void StreamSet::profile_resident(float *ms, int *launches)
@@ -302,14 +411,16 @@ void StreamSet::profile_resident(float *ms, int *launches)
 
 void StreamSet::get_depth(int i, float *out, size_t stride)
 {
+  wait();
   const State &s = st_[i];
-  check(cudaMemcpy2D(out, stride * sizeof(float), eng_->buffers(i).dense, s.d.W * sizeof(float),
+  check(cudaMemcpy2D(out, stride * sizeof(float), device_depth(i), s.d.W * sizeof(float),
                      s.d.W * sizeof(float), s.d.H, cudaMemcpyDeviceToHost),
         "depth download");
 }
 
 void StreamSet::get_debug(int i, float *out, size_t stride)
 {
+  wait();
   const State &s = st_[i];
   check(cudaMemcpy2D(out, stride * sizeof(float), eng_->buffers(i).sparse, s.d.W * sizeof(float),
                      s.d.W * sizeof(float), s.d.H, cudaMemcpyDeviceToHost),
@@ -321,19 +432,27 @@ void StreamSet::get_depths(const int *streams, int n, float *const *outs, const 
   for (int k = 0; k < n; ++k)
     if (streams[k] < 0 || streams[k] >= size() || !outs[k] || strides[k] < (size_t)st_[streams[k]].d.W)
       throw CudaError{QM_ERR_INVALID_ARG, "bad stream index, output pointer or stride"};
+  wait();
   for (int k = 0; k < n; ++k)
   {
     const State &s = st_[streams[k]];
-    check(cudaMemcpy2DAsync(outs[k], strides[k] * sizeof(float), eng_->buffers(streams[k]).dense,
-                            s.d.W * sizeof(float), s.d.W * sizeof(float), s.d.H,
-                            cudaMemcpyDeviceToHost, eng_->stream()),
-          "depth download");
+    const float *src = device_depth(streams[k]);
+    if (strides[k] == (size_t)s.d.W)
+      check(cudaMemcpyAsync(outs[k], src, sizeof(float) * s.d.W * s.d.H, cudaMemcpyDeviceToHost,
+                            eng_->stream()),
+            "depth download");
+    else
+      check(cudaMemcpy2DAsync(outs[k], strides[k] * sizeof(float), src, s.d.W * sizeof(float),
+                              s.d.W * sizeof(float), s.d.H, cudaMemcpyDeviceToHost,
+                              eng_->stream()),
+            "depth download");
   }
   check(cudaStreamSynchronize(eng_->stream()), "depth download");
 }
 
 void StreamSet::get_reference(int i, uint8_t *out, size_t stride)
 {
+  wait();
   const State &s = st_[i];
   if (!s.has_ref)
     throw CudaError{QM_ERR_STATE, "no result yet"};

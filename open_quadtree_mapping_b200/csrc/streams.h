@@ -40,8 +40,19 @@ public:
 
   int size() const { return (int)st_.size(); }
   // One frame per stream (imgs[i] host, pitch strides[i]); has_result out.
+  // Waits for the results.
   void add_frames(const uint8_t *const *imgs, const size_t *strides, const float *T_curr_world,
                   int *has_result);
+  // Pipelined form: runs the frame policy, enqueues the uploads, the dense
+  // pipeline and (where depth_outs[i] is given) the download of stream i's
+  // fused depth, and returns without waiting.  Up to two steps are in
+  // flight: the uploads of step t+1 and the download of step t overlap the
+  // pipeline.  Image buffers may be reused when the next submit (or wait)
+  // returns; depth_outs are complete when wait() returns.
+  void submit(const uint8_t *const *imgs, const size_t *strides, const float *T_curr_world,
+              int *has_result, float *const *depth_outs, const size_t *depth_strides);
+  // Waits for every submitted step.
+  void wait();
   // Single-stream form used by the Depthmap facade.
   int add_frame(int i, const uint8_t *img, size_t stride, const float *T_curr_world);
   void run_resident();
@@ -54,7 +65,10 @@ public:
   void get_depths(const int *streams, int n, float *const *outs, const size_t *strides);
   void get_T_world_ref(int i, float *T) const;
   const StreamDesc &desc(int i) const { return st_[i].d; }
-  const float *device_depth(int i) const { return eng_->buffers(i).dense; }
+  const float *device_depth(int i) const
+  {
+    return eng_->buffers(i).dense[st_[i].out_parity];
+  }
   Engine &engine() { return *eng_; }
   std::mutex &mutex() { return mu_; }
 
@@ -83,11 +97,18 @@ private:
     bool initialized = false;
     Outcome outcome = kSkip;
     bool has_ref = false; // the pool's last slot holds the last result's image
+    int out_parity = 0;   // output buffer of the last result
     SE3f T_world_ref;
   };
 
   Outcome begin_frame(int i, const uint8_t *img, size_t stride, const float *T);
-  void end_frame(int i);
+  void end_frame(int i, int parity);
+  // one step of the streams in `which` (see submit)
+  void step(const std::vector<int> &which, const uint8_t *const *imgs, const size_t *strides,
+            const float *T_curr_world, int *has_result, float *const *depth_outs,
+            const size_t *depth_strides);
+  // waits for the step of parity p and recycles the frame slots it freed
+  void retire(int p);
   bool need_add_reference(const State &s) const;
   bool need_switch_keyframe(const State &s) const;
   uint8_t *frame_ptr(const State &s, int slot) const
@@ -102,6 +123,14 @@ private:
   std::unique_ptr<Engine> eng_;
   std::vector<int> last_active_;
   std::mutex mu_;
+  // pipelining: uploads and downloads run on their own streams; per step
+  // parity, events mark the end of its uploads, of its pipeline and of its
+  // downloads, and the frame slots it freed wait in `pending_` until then
+  cudaStream_t up_ = nullptr, down_ = nullptr;
+  cudaEvent_t ev_up_[2] = {}, ev_comp_[2] = {}, ev_done_[2] = {};
+  std::vector<std::pair<int, int>> pending_[2]; // (stream, slot)
+  bool inflight_[2] = {false, false};
+  long step_ = 0;
 };
 
 } // namespace qm

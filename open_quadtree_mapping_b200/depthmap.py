@@ -170,6 +170,43 @@ class BatchDepthmap:
         _lib.check(_lib.lib().qm_batch_add_frames(self._h, ptrs, strides, T.ctypes.data, has))
         return [bool(h) for h in has]
 
+    def submit(self, imgs, poses, outs=None):
+        """Pipelined add_frames (qm_batch_submit): returns the n booleans at
+        once; the depth of every stream with a result is downloaded into
+        outs[i] (float32 (H, W), ideally pinned) and is complete after
+        wait().  Image arrays must stay unchanged until the next submit or
+        wait returns."""
+        n = self.n
+        ptrs = (ctypes.c_void_p * n)()
+        strides = (ctypes.c_size_t * n)()
+        keep = []
+        for i, im in enumerate(imgs):
+            a = np.asarray(im)
+            if a.dtype != np.uint8 or a.shape != self.shapes[i] or a.strides[1] != 1:
+                a = np.ascontiguousarray(a, dtype=np.uint8)
+            keep.append(a)
+            ptrs[i] = a.ctypes.data
+            strides[i] = a.strides[0]
+        dptrs = dstrides = None
+        if outs is not None:
+            for i, o in enumerate(outs):
+                if o.dtype != np.float32 or o.shape != tuple(self.shapes[i]) or o.strides[1] != 4:
+                    raise ValueError("output %d must be a float32 %s array" % (i, self.shapes[i]))
+            dptrs = (ctypes.c_void_p * n)(*[o.ctypes.data for o in outs])
+            dstrides = (ctypes.c_size_t * n)(*[o.strides[0] // 4 for o in outs])
+            keep.extend(outs)
+        T = np.ascontiguousarray(np.stack([_pose12(p) for p in poses]), dtype=np.float32)
+        has = (ctypes.c_int * n)()
+        _lib.check(_lib.lib().qm_batch_submit(self._h, ptrs, strides, T.ctypes.data, has,
+                                              dptrs, dstrides))
+        # the buffers of the last two steps may still be in use on the device
+        self._inflight = (getattr(self, "_inflight", (None, None))[1], keep)
+        return [bool(h) for h in has]
+
+    def wait(self) -> None:
+        _lib.check(_lib.lib().qm_batch_wait(self._h))
+        self._inflight = (None, None)
+
     def get_depth(self, i, out: np.ndarray | None = None) -> np.ndarray:
         H, W = self.shapes[i]
         if out is None:

@@ -106,6 +106,40 @@ def test_batch_equals_plain_and_graph_equals_eager(gpu):
     assert batch.last_launches() > 0
 
 
+def test_submit_pipeline_equals_add_frames(gpu):
+    """qm_batch_submit (two steps in flight, uploads and downloads on their
+    own streams) gives the same flags and bit-identical depth maps as the
+    synchronous add_frames + get_depths, frame by frame."""
+    from open_quadtree_mapping_b200.depthmap import BatchDepthmap
+    seqs = [sequence(s, 16, W, H) for s in (5, 6, 7)]
+    p = Params.for_range(64, 0.5, 50.0)
+    sync = BatchDepthmap([_stream_kw()] * 3, params=p)
+    pipe = BatchDepthmap([_stream_kw()] * 3, params=p)
+    want, got = [], []
+    for i in range(16):
+        imgs = [s[0][i] for s in seqs]
+        poses = [s[1][i] for s in seqs]
+        hs = sync.add_frames(imgs, poses)
+        want.append((hs, [d.copy() for d in sync.get_depths()]))
+        outs = [np.full((H, W), np.nan, np.float32) for _ in range(3)]
+        hp = pipe.submit(imgs, poses, outs=outs)
+        got.append((hp, outs))
+    pipe.wait()
+    for (hs, ds), (hp, outs) in zip(want, got):
+        assert hs == hp
+        for k in range(3):
+            if hp[k]:
+                assert np.array_equal(ds[k], outs[k])
+            else:
+                assert np.isnan(outs[k]).all()  # nothing downloaded
+    # the synchronous getters wait for submitted work by themselves
+    imgs = [s[0][15] for s in seqs]
+    pipe.submit(imgs, [s[1][15] for s in seqs])
+    sync.add_frames(imgs, [s[1][15] for s in seqs])
+    for k in range(3):
+        assert np.array_equal(pipe.get_depth(k), sync.get_depth(k))
+
+
 def test_uneven_batch_equals_per_stream(gpu):
     """Streams of different sizes, hypothesis and slot counts in one batch."""
     from open_quadtree_mapping_b200.depthmap import BatchDepthmap
