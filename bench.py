@@ -75,6 +75,7 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.path = None
+        self.skip = 0
 
     def __enter__(self):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
@@ -82,11 +83,31 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.QUERY,
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "25"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
         return self
+
+    def wait_first_sample(self, timeout=3.0):
+        """Blocks until the sampler has written a line (nvidia-smi start-up
+        takes a moment), so that the timed region that follows is sampled."""
+        t0 = time.time()
+        while self.proc is not None and time.time() - t0 < timeout:
+            try:
+                if os.path.getsize(self.path) > 0:
+                    return
+            except OSError:
+                pass
+            time.sleep(0.02)
+
+    def mark(self):
+        """Samples written before this call are left out of the summary."""
+        try:
+            with open(self.path) as f:
+                self.skip = sum(1 for _ in f)
+        except Exception:
+            self.skip = 0
 
     def __exit__(self, *exc):
         if self.proc is not None:
@@ -99,7 +120,10 @@ class ClockSampler:
     def summary(self):
         rows = []
         try:
-            for line in open(self.path):
+            lines = open(self.path).readlines()
+            # the samples of the timed region (and the last one before it, so
+            # that a short region still has one)
+            for line in lines[max(0, self.skip - 1):]:
                 f = [x.strip() for x in line.split(",")]
                 if len(f) >= 9:
                     rows.append(f)
@@ -189,6 +213,24 @@ def algorithmic_bytes(levels_list, params):
         by["fuse_fill"] += P * 12
         by["fuse_update"] += P * 52
     return by
+
+
+def dram_traffic(kind, streams):
+    """DRAM bytes (read + write) per launch of kernel kind `kind` from the
+    committed ncu capture of this workload (profiles/), scaled by the stream
+    count when the bench runs a different one.  (None, reason) if absent."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic_752x480x64_32streams.json")
+    try:
+        with open(path) as f:
+            cap = json.load(f)
+        per = cap["kernels"][kind]["dram_bytes_per_launch"]
+    except Exception:
+        return None, "no capture for this kernel"
+    scale = streams / float(cap["streams"])
+    src = "ncu capture, %d streams (profiles/%s)" % (cap["streams"], os.path.basename(path))
+    if scale != 1.0:
+        src += ", scaled by %d/%d streams" % (streams, cap["streams"])
+    return int(per * scale), src
 
 
 def cpu_baseline(kf_imgs, kf_Ts, budget_s=12.0):
@@ -374,6 +416,8 @@ def main():
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
+        clk.wait_first_sample()
+        clk.mark()
         e0.record(ext)
         for _ in range(args.steps):
             batch.run_resident()
@@ -430,11 +474,14 @@ def main():
     dom = max(prof, key=lambda k: prof[k][0])
     dms, dn = prof[dom]
     achieved = alg[dom] / (dms * 1e-3) / 1e9
+    traffic, traffic_src = dram_traffic(dom, S)
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
-                "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
-                "peak_source": peak_kind,
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                "traffic_source": traffic_src, "peak_source": peak_kind,
                 "per_launch_alg_bytes": alg[dom] / max(dn, 1),
-                "avg_launch_ms": dms / max(dn, 1)}
+                "avg_launch_ms": dms / max(dn, 1),
+                "timing": "CUDA events around every launch of one eager run on the "
+                          "library's stream, right after the timed region"}
 
     # ---- plain per-frame path: one stream, launched stage by stage
     plain = BatchDepthmap([desc], params=params, device=local)

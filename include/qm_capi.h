@@ -109,6 +109,10 @@ int qm_depthmap_add_frame(qm_depthmap *h, const uint8_t *img, size_t stride,
 int qm_depthmap_get_depth(qm_depthmap *h, float *out, size_t stride);
 /* getDebugmap (depthmap.h:50): the sparse depth handed to the upsampler. */
 int qm_depthmap_get_debug(qm_depthmap *h, float *out, size_t stride);
+/* Fused variance sigma^2 per pixel of the last result (the fourth component
+ * of the Bayesian seeds after fuse_currentmap, depth_fusion.cu:199-205); the
+ * reference's Depthmap has no getter for it.  stride in elements. */
+int qm_depthmap_get_variance(qm_depthmap *h, float *out, size_t stride);
 /* getReferenceImage (depthmap.h:51): the image the last depth map belongs to. */
 int qm_depthmap_get_reference(qm_depthmap *h, uint8_t *out, size_t stride);
 /* getT_world_ref (depthmap.h:74). */
@@ -155,6 +159,7 @@ int qm_batch_submit(qm_batch *b, const uint8_t *const *imgs, const size_t *strid
 int qm_batch_wait(qm_batch *b);
 int qm_batch_get_depth(qm_batch *b, int stream, float *out, size_t stride);
 int qm_batch_get_debug(qm_batch *b, int stream, float *out, size_t stride);
+int qm_batch_get_variance(qm_batch *b, int stream, float *out, size_t stride);
 /* Fused depth of n streams in one call: streams[k] is written to outs[k]
  * (row pitch strides[k] elements); the downloads are issued together and
  * waited for once. */

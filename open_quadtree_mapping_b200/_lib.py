@@ -65,6 +65,7 @@ _SIGS = {
     "qm_depthmap_get_depth": (_I, [_P, _P, _S]),
     "qm_depthmap_get_debug": (_I, [_P, _P, _S]),
     "qm_depthmap_get_reference": (_I, [_P, _P, _S]),
+    "qm_depthmap_get_variance": (_I, [_P, _P, _S]),
     "qm_depthmap_get_T_world_ref": (_I, [_P, _P]),
     "qm_depthmap_get_camera": (_I, [_P, ctypes.POINTER(QmCamera), ctypes.POINTER(_I),
                                     ctypes.POINTER(_I)]),
@@ -76,6 +77,7 @@ _SIGS = {
     "qm_batch_submit": (_I, [_P, _P, _P, _P, _P, _P, _P]),
     "qm_batch_wait": (_I, [_P]),
     "qm_batch_get_debug": (_I, [_P, _I, _P, _S]),
+    "qm_batch_get_variance": (_I, [_P, _I, _P, _S]),
     "qm_batch_get_depths": (_I, [_P, _I, _P, _P, _P]),
     "qm_batch_run_resident": (_I, [_P]),
     "qm_batch_device_depth": (_I, [_P, _I, ctypes.POINTER(_P)]),

@@ -243,6 +243,15 @@ int qm_depthmap_get_debug(qm_depthmap *h, float *out, size_t stride)
   });
 }
 
+int qm_depthmap_get_variance(qm_depthmap *h, float *out, size_t stride)
+{
+  return guarded([&] {
+    require(h && out && stride >= (size_t)h->width, "bad argument");
+    std::lock_guard<std::mutex> lock(h->set->mutex());
+    h->set->get_variance(0, out, stride);
+  });
+}
+
 int qm_depthmap_get_reference(qm_depthmap *h, uint8_t *out, size_t stride)
 {
   return guarded([&] {
@@ -364,6 +373,17 @@ int qm_batch_run_resident(qm_batch *b)
     require(b != nullptr, "NULL handle");
     std::lock_guard<std::mutex> lock(b->set->mutex());
     b->set->run_resident();
+  });
+}
+
+int qm_batch_get_variance(qm_batch *b, int stream, float *out, size_t stride)
+{
+  return guarded([&] {
+    require(b && out && stream >= 0 && stream < b->set->size() &&
+                stride >= (size_t)b->set->desc(stream).W,
+            "bad argument");
+    std::lock_guard<std::mutex> lock(b->set->mutex());
+    b->set->get_variance(stream, out, stride);
   });
 }
 

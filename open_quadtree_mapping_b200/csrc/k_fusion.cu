@@ -136,28 +136,53 @@ __global__ void __launch_bounds__(kFlatThreads)
     mu = dep;
     s2 = 2500.0;
   }
+  // The reference's formulas with each shared denominator inverted once (FP64
+  // division is the costly operation here); the results differ from the
+  // term-by-term quotients by a few FP64 ulps.  The inlier ratio that gates
+  // the output is the exact quotient.
   const double var = unc + s2;
-  const double new_sq = unc * s2 / var;
-  const double new_mu = (dep * s2 + mu * unc) / var;
-  const double pdf = exp(-(dep - mu) * (dep - mu) / (2.0 * var)) / sqrt(2.0 * M_PI * var);
-  double c1 = (a / (a + b)) * pdf;
-  double c2 = (b / (a + b)) / 50.0;
-  const double norm = c1 + c2;
-  c1 /= norm;
-  c2 /= norm;
-  const double f = c1 * ((a + 1.0) / (a + b + 1.0)) + c2 * (a / (a + b + 1.0));
-  const double e = c1 * (((a + 1.0) * (a + 2.0)) / ((a + b + 1.0) * (a + b + 2.0))) +
-                   c2 * (a * (a + 1.0) / ((a + b + 1.0) * (a + b + 2.0)));
+  const double ivar = 1.0 / var;
+  const double new_sq = unc * s2 * ivar;
+  const double new_mu = (dep * s2 + mu * unc) * ivar;
+  const double dm = dep - mu;
+  const double pdf = exp(-dm * dm * (0.5 * ivar)) * rsqrt(2.0 * M_PI * var);
+  const double ab = a + b;
+  const double ratio = a / ab;
+  double c1 = ratio * pdf;
+  double c2 = b * (1.0 / ab) * (1.0 / 50.0);
+  const double inorm = 1.0 / (c1 + c2);
+  c1 *= inorm;
+  c2 *= inorm;
+  const double i1 = 1.0 / (ab + 1.0), i2 = 1.0 / (ab + 2.0);
+  const double f = (c1 * (a + 1.0) + c2 * a) * i1;
+  const double e = (c1 * ((a + 1.0) * (a + 2.0)) + c2 * (a * (a + 1.0))) * (i1 * i2);
   const double mu_p = c1 * new_mu + c2 * mu;
   const double s2_p = c1 * (new_sq + new_mu * new_mu) + c2 * (s2 + mu * mu) - mu_p * mu_p;
-  const double a_p = (e - f) / (f - e / f);
-  const double b_p = a_p * (1.0 - f) / f;
-  J.dense[idx] = (a / (a + b) > 0.60) ? (float)mu_p : -1.0f;
+  const double inv_f = 1.0 / f;
+  const double a_p = (e - f) / (f - e * inv_f);
+  const double b_p = a_p * (1.0 - f) * inv_f;
+  J.dense[idx] = (ratio > 0.60) ? (float)mu_p : -1.0f;
   J.seeds_out[idx] = make_float4((float)a_p, (float)b_p, (float)mu_p, (float)s2_p);
   J.zkey[idx] = kEmpty;
 }
 
+// sigma^2 of every seed (the fused variance)
+__global__ void __launch_bounds__(kFlatThreads)
+    k_seed_variance(const float4 *__restrict__ seeds, float *__restrict__ out, long n)
+{
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n)
+    out[i] = seeds[i].w;
+}
+
 } // namespace
+
+void launch_seed_variance(const float4 *seeds, float *out, long n, cudaStream_t s)
+{
+  if (n > 0)
+    k_seed_variance<<<(unsigned)((n + kFlatThreads - 1) / kFlatThreads), kFlatThreads, 0, s>>>(
+        seeds, out, n);
+}
 
 void launch_fuse_transform(const Batch &B, int blocks, int arith, cudaStream_t s)
 {

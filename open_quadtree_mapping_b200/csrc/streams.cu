@@ -418,6 +418,21 @@ void StreamSet::get_depth(int i, float *out, size_t stride)
         "depth download");
 }
 
+void StreamSet::get_variance(int i, float *out, size_t stride)
+{
+  wait();
+  const State &s = st_[i];
+  const size_t P = (size_t)s.d.W * s.d.H;
+  // the row-pass buffer is idle between runs: stage the variances there
+  float *tmp = reinterpret_cast<float *>(eng_->buffers(i).rowres);
+  launch_seed_variance(eng_->seeds(i), tmp, (long)P, eng_->stream());
+  check(cudaGetLastError(), "variance extraction");
+  check(cudaMemcpy2DAsync(out, stride * sizeof(float), tmp, s.d.W * sizeof(float),
+                          s.d.W * sizeof(float), s.d.H, cudaMemcpyDeviceToHost, eng_->stream()),
+        "variance download");
+  check(cudaStreamSynchronize(eng_->stream()), "variance download");
+}
+
 void StreamSet::get_debug(int i, float *out, size_t stride)
 {
   wait();

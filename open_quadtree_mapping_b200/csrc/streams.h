@@ -60,6 +60,8 @@ public:
 
   void get_depth(int i, float *out, size_t stride);
   void get_debug(int i, float *out, size_t stride);
+  // fused variance sigma^2 of every pixel of the last result
+  void get_variance(int i, float *out, size_t stride);
   void get_reference(int i, uint8_t *out, size_t stride);
   // fused depth of several streams: all downloads enqueued, one wait
   void get_depths(const int *streams, int n, float *const *outs, const size_t *strides);

@@ -85,6 +85,12 @@ class Depthmap:
         _lib.check(_lib.lib().qm_depthmap_get_debug(self._h, out.ctypes.data, self.width))
         return out
 
+    def getVariancemap(self) -> np.ndarray:
+        """Fused variance sigma^2 per pixel of the last result."""
+        out = np.empty((self.height, self.width), np.float32)
+        _lib.check(_lib.lib().qm_depthmap_get_variance(self._h, out.ctypes.data, self.width))
+        return out
+
     def getReferenceImage(self) -> np.ndarray:
         out = np.empty((self.height, self.width), np.uint8)
         _lib.check(_lib.lib().qm_depthmap_get_reference(self._h, out.ctypes.data, self.width))
@@ -231,6 +237,13 @@ class BatchDepthmap:
         strides = (ctypes.c_size_t * n)(*[o.strides[0] // 4 for o in outs])
         _lib.check(_lib.lib().qm_batch_get_depths(self._h, n, idx, ptrs, strides))
         return outs
+
+    def get_variance(self, i) -> np.ndarray:
+        """Fused variance sigma^2 per pixel of stream i's last result."""
+        H, W = self.shapes[i]
+        out = np.empty((H, W), np.float32)
+        _lib.check(_lib.lib().qm_batch_get_variance(self._h, i, out.ctypes.data, W))
+        return out
 
     def get_debug(self, i) -> np.ndarray:
         H, W = self.shapes[i]

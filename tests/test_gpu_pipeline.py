@@ -54,6 +54,13 @@ def test_facade_matches_oracle_replay(oracle_mod, gpu):
         depth = dm.getDepthmap()
         valid = fused > 0
         n_oracle_valid += valid.sum()
+        # fused variance: sigma^2 of the new seeds where both fused the pixel
+        var = dm.getVariancemap()
+        ok = valid & (depth > 0)
+        if ok.any():
+            ov = new_seeds[..., 3][ok]
+            rel = np.abs(var[ok] - ov) / np.maximum(np.abs(ov), 1e-6)
+            assert np.percentile(rel, 99) < 1e-4, np.percentile(rel, 99)
         assert (depth > 0).mean() == pytest.approx(valid.mean(), abs=2e-3)
         both = valid & (depth > 0)
         n_valid += both.sum()
