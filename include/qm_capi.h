@@ -267,6 +267,48 @@ int qm_fuse(float *depth, float *seeds_in, float *seeds_out, const float T_incom
             const qm_camera *cam, int width, int height, const qm_params *p, int32_t *table,
             void *workspace, size_t workspace_bytes, void *stream);
 
+/* ------------------------------------------------- differentiable path ----
+ * For fitting the BP penalties (P1, P2) and per-pixel upsampling weight
+ * factors to ground-truth depth.  No counterpart in the reference: it is the
+ * training-side use of the stages above (the plain path keeps the hard
+ * argmin).  Device pointers, asynchronous on `stream`.
+ *
+ * Soft BP: the hierarchical BP of qm_bp_extract followed by a softened
+ * readout at the node cells: p(d) = softmax(-belief(d) / tau), depth =
+ * 1 / (inv_depth_step * sum p(d) d + min_inv_depth), written at (4x, 4y) of
+ * every node cell of `sparse` (zero elsewhere).  qm_bp_soft_backward takes
+ * the same inputs, the workspace as the forward left it, and dL/d sparse,
+ * and writes dL/dP1, dL/dP2 to grad_penalties (2 device doubles); it
+ * recomputes the messages of each level instead of storing all of them.
+ * cost and workspace 16-byte aligned. */
+int qm_bp_soft_workspace_size(int width, int height, const qm_params *p, size_t *bytes);
+int qm_bp_soft_forward(const float *cost, int width, int height, const uint8_t *levels,
+                       const qm_params *p, float tau, float *sparse, void *workspace,
+                       size_t workspace_bytes, void *stream);
+int qm_bp_soft_backward(const float *cost, int width, int height, const uint8_t *levels,
+                        const qm_params *p, float tau, const float *grad_sparse,
+                        double *grad_penalties, void *workspace, size_t workspace_bytes,
+                        void *stream);
+/* Upsampling with a weight factor per pixel: the systems of qm_upsample with
+ * every inner edge weight (between a pixel and its left or upper neighbour)
+ * multiplied by omega at that pixel, solved per line in FP64.  The backward
+ * takes the forward's workspace unchanged and writes dL/d sparse and
+ * dL/d omega.  width % 16 == 0, height % 8 == 0. */
+int qm_upsample_w_workspace_size(int width, int height, size_t *bytes);
+int qm_upsample_w_forward(const float *sparse, const uint8_t *img, size_t img_pitch, int width,
+                          int height, const qm_params *p, const float *omega, float *dense,
+                          void *workspace, size_t workspace_bytes, void *stream);
+int qm_upsample_w_backward(const uint8_t *img, size_t img_pitch, int width, int height,
+                           const qm_params *p, const float *omega, const float *grad_dense,
+                           float *grad_sparse, float *grad_omega, void *workspace,
+                           size_t workspace_bytes, void *stream);
+/* Adjoint of the fusion update (fuse_currentmap) with respect to the
+ * upsampled depth: depth_in = the depth qm_fuse was given, seeds_in = the
+ * seeds as qm_fuse left them (transformed), table = its table. */
+int qm_fuse_backward(const float *depth_in, const float *seeds_in, const int32_t *table,
+                     int width, int height, const float *grad_fused, float *grad_depth,
+                     void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -97,6 +97,16 @@ _SIGS = {
     "qm_fuse_workspace_size": (_I, [_I, _I, ctypes.POINTER(_S)]),
     "qm_fuse": (_I, [_P, _P, _P, _P, ctypes.POINTER(QmCamera), _I, _I,
                      ctypes.POINTER(QmParamsC), _P, _P, _S, _P]),
+    "qm_bp_soft_workspace_size": (_I, [_I, _I, ctypes.POINTER(QmParamsC), ctypes.POINTER(_S)]),
+    "qm_bp_soft_forward": (_I, [_P, _I, _I, _P, ctypes.POINTER(QmParamsC), _F, _P, _P, _S, _P]),
+    "qm_bp_soft_backward": (_I, [_P, _I, _I, _P, ctypes.POINTER(QmParamsC), _F, _P, _P, _P, _S,
+                                 _P]),
+    "qm_upsample_w_workspace_size": (_I, [_I, _I, ctypes.POINTER(_S)]),
+    "qm_upsample_w_forward": (_I, [_P, _P, _S, _I, _I, ctypes.POINTER(QmParamsC), _P, _P, _P,
+                                   _S, _P]),
+    "qm_upsample_w_backward": (_I, [_P, _S, _I, _I, ctypes.POINTER(QmParamsC), _P, _P, _P, _P,
+                                    _P, _S, _P]),
+    "qm_fuse_backward": (_I, [_P, _P, _P, _I, _I, _P, _P, _P]),
 }
 
 

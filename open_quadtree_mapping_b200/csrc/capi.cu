@@ -1,6 +1,7 @@
 // extern "C" entry points of libqm_b200.so (declared in include/qm_capi.h).
 // Every entry point catches all exceptions and returns a status code; the
 // message is kept per thread for qm_last_error().
+#include <algorithm>
 #include <cstring>
 #include <new>
 
@@ -149,6 +150,212 @@ void run_stage(const qm::JobDesc &J, const qm_params &p, const qm::Shape &s, con
     B.slots = *slots;
   qm::stage::run_range(B, s, p, qm::stage::first_of(name, p.bp_levels),
                        qm::stage::last_of(name, p.bp_levels), as_stream(stream));
+}
+
+// Workspace of the soft BP: the BP workspace of qm_bp_extract (pyramid data
+// and messages of every level), the message states of one level's half-sweeps
+// for the adjoint (sized for the largest level: iterations + 1 states), and
+// two adjoint buffers of the level-0 size.
+struct SoftLayout
+{
+  size_t bp = 0, hist = 0, dir = 0, total = 0;
+};
+
+SoftLayout soft_layout(int W, int H, const qm_params &p)
+{
+  SoftLayout L;
+  L.bp = bp_workspace(W, H, p);
+  int w = W / 4, h = H / 4;
+  L.dir = align256((size_t)w * h * p.num_hyp * sizeof(float));
+  for (int l = 0; l < p.bp_levels; ++l)
+  {
+    const size_t n = align256((size_t)w * h * p.num_hyp * sizeof(float));
+    L.hist = std::max(L.hist, (size_t)(p.bp_iters[l] + 1) * 4 * n);
+    w = (w + 1) / 2;
+    h = (h + 1) / 2;
+  }
+  L.total = L.bp + L.hist + 2 * 4 * L.dir;
+  return L;
+}
+
+int cdiv_i(long a, long b) { return (int)((a + b - 1) / b); }
+
+// Soft BP of one keyframe over a caller workspace (see SoftLayout).
+struct SoftBp
+{
+  qm::JobDesc J;
+  SoftLayout lay;
+  char *hist = nullptr, *adj[2] = {nullptr, nullptr};
+
+  SoftBp(const float *cost, int W, int H, const uint8_t *levels, const qm_params &q, void *ws,
+         size_t bytes)
+  {
+    lay = soft_layout(W, H, q);
+    if (!ws || bytes < lay.total)
+      throw CudaError{QM_ERR_WORKSPACE, "soft BP workspace too small"};
+    require(((uintptr_t)cost | (uintptr_t)ws) % 16 == 0,
+            "cost and workspace must be 16-byte aligned");
+    J = base_desc(W, H, q);
+    J.levels = const_cast<uint8_t *>(levels);
+    char *b = (char *)ws;
+    size_t o = 0;
+    int w = W / 4, h = H / 4;
+    for (int l = 0; l < q.bp_levels; ++l)
+    {
+      const size_t n = (size_t)w * h * q.num_hyp * sizeof(float);
+      J.lv[l].w = w;
+      J.lv[l].h = h;
+      if (l == 0)
+        J.lv[l].data = const_cast<float *>(cost);
+      else
+      {
+        J.lv[l].data = (float *)(b + o);
+        o += align256(n);
+      }
+      for (int m = 0; m < 4; ++m)
+      {
+        J.lv[l].msg[m] = (float *)(b + o);
+        o += align256(n);
+      }
+      w = (w + 1) / 2;
+      h = (h + 1) / 2;
+    }
+    hist = b + lay.bp;
+    adj[0] = hist + lay.hist;
+    adj[1] = adj[0] + 4 * lay.dir;
+  }
+
+  qm::DiffBp level_args(int l, const qm_params &q, float tau) const
+  {
+    qm::DiffBp a;
+    std::memset(&a, 0, sizeof(a));
+    a.W = J.W;
+    a.H = J.H;
+    a.D = q.num_hyp;
+    a.w = J.lv[l].w;
+    a.h = J.lv[l].h;
+    a.level = l;
+    a.qt_max = q.qt_max_level;
+    a.levels = J.levels;
+    a.data = J.lv[l].data;
+    for (int m = 0; m < 4; ++m)
+      a.S[m] = J.lv[l].msg[m];
+    a.P1 = q.P1;
+    a.P2 = q.P2;
+    a.tau = tau;
+    a.step = q.inv_depth_step;
+    a.min_inv = q.min_inv_depth;
+    return a;
+  }
+
+  qm::MsgPtrs adjoint(int buf) const
+  {
+    qm::MsgPtrs p;
+    for (int m = 0; m < 4; ++m)
+      p.m[m] = (float *)(adj[buf] + m * lay.dir);
+    return p;
+  }
+
+  // Reverse mode over the whole pyramid, fine to coarse: the readout's
+  // adjoint enters at level 0; every level recomputes its half-sweeps from
+  // its starting state (all cells inherit the parents' final messages),
+  // keeping each state, then runs the half-sweep adjoints backwards and hands
+  // the adjoint of its starting state to the parents.
+  void backward(const qm_params &q, float tau, const float *g_sparse, double *gP,
+                cudaStream_t s)
+  {
+    const int L = q.bp_levels, D = q.num_hyp;
+    const qm::KParams kp = qm::kparams(q);
+    qm::check(cudaMemsetAsync(gP, 0, 2 * sizeof(double), s), "memset");
+    int cur = 0;
+    qm::check(cudaMemsetAsync(adj[cur], 0, 4 * lay.dir, s), "memset");
+    {
+      qm::DiffBp a = level_args(0, q, tau);
+      const qm::MsgPtrs A = adjoint(cur);
+      for (int m = 0; m < 4; ++m)
+        a.A[m] = A.m[m];
+      a.g_sparse = g_sparse;
+      qm::launch_soft_readout(a, 1, s);
+    }
+    const qm::Batch B = qm::stage::single(J);
+    for (int l = 0; l < L; ++l)
+    {
+      const int w = J.lv[l].w, h = J.lv[l].h;
+      const size_t n = (size_t)w * h * D;
+      const size_t slot = align256(n * sizeof(float));
+      auto state = [&](int i, int m) { return (float *)(hist + ((size_t)i * 4 + m) * slot); };
+      auto snapshot = [&](int i) {
+        for (int m = 0; m < 4; ++m)
+          qm::check(cudaMemcpyAsync(state(i, m), J.lv[l].msg[m], n * sizeof(float),
+                                    cudaMemcpyDeviceToDevice, s),
+                    "message snapshot");
+      };
+      qm::launch_msg_inherit(B, cdiv_i((long)w * h * (D / 4), qm::kFlatThreads), l, 0,
+                             q.qt_max_level, s);
+      snapshot(0);
+      const int sweep_blocks =
+          cdiv_i((long)((w + 1) / 2) * h, qm::kCellWarps * qm::bp_cells_per_warp(D));
+      const int it = q.bp_iters[l];
+      for (int i = 0; i < it; ++i)
+      {
+        qm::launch_bp_sweep_own(B, sweep_blocks, D, l, i & 1, kp, q.arith, s);
+        snapshot(i + 1);
+      }
+      const qm::MsgPtrs A = adjoint(cur);
+      for (int i = it - 1; i >= 0; --i)
+      {
+        qm::DiffBp a = level_args(l, q, tau);
+        for (int m = 0; m < 4; ++m)
+        {
+          a.S[m] = state(i, m);
+          a.A[m] = A.m[m];
+        }
+        a.parity = i & 1;
+        a.gP = gP;
+        qm::launch_bp_sweep_bwd(a, s);
+      }
+      if (l + 1 < L)
+      {
+        const int pw = J.lv[l + 1].w, ph = J.lv[l + 1].h;
+        const qm::MsgPtrs P = adjoint(cur ^ 1);
+        for (int m = 0; m < 4; ++m)
+          qm::check(cudaMemsetAsync(P.m[m], 0, (size_t)pw * ph * D * sizeof(float), s),
+                    "memset");
+        qm::launch_msg_downsample_add(A, w, h, P, pw, ph, D, s);
+        cur ^= 1;
+      }
+    }
+    qm::check(cudaGetLastError(), "soft BP adjoint");
+  }
+};
+
+qm::DiffUp upw_args(const uint8_t *img, size_t pitch, int W, int H, const qm_params *p,
+                    const float *omega, void *ws, size_t bytes)
+{
+  check_stage_size(W, H);
+  require(W % 16 == 0 && H % 8 == 0, "width must be a multiple of 16 and height of 8");
+  require(img && omega && pitch >= (size_t)W, "bad argument");
+  const qm_params q = params_or_default(p);
+  const size_t one = align256((size_t)W * H * sizeof(double));
+  if (!ws || bytes < 7 * one)
+    throw CudaError{QM_ERR_WORKSPACE, "weighted upsampling workspace too small"};
+  qm::DiffUp u;
+  std::memset(&u, 0, sizeof(u));
+  u.W = W;
+  u.H = H;
+  u.img = img;
+  u.pitch = pitch;
+  u.omega = omega;
+  u.lam = q.up_lambda;
+  u.sigma = q.up_sigma;
+  // the reference's closing weights (depth_upsample.cu:26-37)
+  u.row_closing = W % 16 != 0 ? 1.0 : 0.0;
+  u.col_closing = H % 16 != 0 ? 1.0 : 0.0;
+  char *b = (char *)ws;
+  double **bufs[7] = {&u.sd, &u.si, &u.td, &u.ti, &u.cp, &u.ud, &u.ui};
+  for (int k = 0; k < 7; ++k)
+    *bufs[k] = (double *)(b + k * one);
+  return u;
 }
 
 } // namespace
@@ -621,6 +828,112 @@ int qm_fuse(float *depth, float *seeds_in, float *seeds_out, const float T_incom
     qm::check(cudaMemsetAsync(workspace, 0xff, fuse_workspace(width, height), as_stream(stream)),
               "workspace reset");
     run_stage(J, q, stage_shape(width, height, q, 1, cam), "fuse", stream);
+  });
+}
+
+// ------------------------------------------------------ differentiable path
+
+int qm_bp_soft_workspace_size(int width, int height, const qm_params *p, size_t *bytes)
+{
+  return guarded([&] {
+    check_stage_size(width, height);
+    require(bytes != nullptr, "NULL argument");
+    *bytes = soft_layout(width, height, params_or_default(p)).total;
+  });
+}
+
+int qm_bp_soft_forward(const float *cost, int width, int height, const uint8_t *levels,
+                       const qm_params *p, float tau, float *sparse, void *workspace,
+                       size_t workspace_bytes, void *stream)
+{
+  return guarded([&] {
+    check_stage_size(width, height);
+    require(cost && levels && sparse && tau > 0.0f, "NULL argument or tau <= 0");
+    const qm_params q = params_or_default(p);
+    SoftBp sb(cost, width, height, levels, q, workspace, workspace_bytes);
+    const cudaStream_t s = as_stream(stream);
+    qm::check(cudaMemsetAsync(sparse, 0, sizeof(float) * width * height, s), "memset");
+    sb.J.sparse = sparse;
+    // hierarchical BP (its hard extraction is overwritten by the soft readout)
+    run_stage(sb.J, q, stage_shape(width, height, q, 1, nullptr), "bp", stream);
+    qm::DiffBp a = sb.level_args(0, q, tau);
+    a.sparse = sparse;
+    qm::launch_soft_readout(a, 0, s);
+    qm::check(cudaGetLastError(), "soft readout");
+  });
+}
+
+int qm_bp_soft_backward(const float *cost, int width, int height, const uint8_t *levels,
+                        const qm_params *p, float tau, const float *grad_sparse,
+                        double *grad_penalties, void *workspace, size_t workspace_bytes,
+                        void *stream)
+{
+  return guarded([&] {
+    check_stage_size(width, height);
+    require(cost && levels && grad_sparse && grad_penalties && tau > 0.0f,
+            "NULL argument or tau <= 0");
+    const qm_params q = params_or_default(p);
+    SoftBp sb(cost, width, height, levels, q, workspace, workspace_bytes);
+    sb.backward(q, tau, grad_sparse, grad_penalties, as_stream(stream));
+  });
+}
+
+int qm_upsample_w_workspace_size(int width, int height, size_t *bytes)
+{
+  return guarded([&] {
+    check_stage_size(width, height);
+    require(bytes != nullptr, "NULL argument");
+    *bytes = align256((size_t)width * height * sizeof(double)) * 7;
+  });
+}
+
+int qm_upsample_w_forward(const float *sparse, const uint8_t *img, size_t img_pitch, int width,
+                          int height, const qm_params *p, const float *omega, float *dense,
+                          void *workspace, size_t workspace_bytes, void *stream)
+{
+  return guarded([&] {
+    qm::DiffUp u = upw_args(img, img_pitch, width, height, p, omega, workspace, workspace_bytes);
+    require(sparse && dense, "NULL argument");
+    u.sparse = sparse;
+    u.dense = dense;
+    qm::launch_upw_forward(u, as_stream(stream));
+    qm::check(cudaGetLastError(), "weighted upsampling");
+  });
+}
+
+int qm_upsample_w_backward(const uint8_t *img, size_t img_pitch, int width, int height,
+                           const qm_params *p, const float *omega, const float *grad_dense,
+                           float *grad_sparse, float *grad_omega, void *workspace,
+                           size_t workspace_bytes, void *stream)
+{
+  return guarded([&] {
+    qm::DiffUp u = upw_args(img, img_pitch, width, height, p, omega, workspace, workspace_bytes);
+    require(grad_dense && grad_sparse && grad_omega, "NULL argument");
+    u.g_dense = grad_dense;
+    u.g_sparse = grad_sparse;
+    u.g_omega = grad_omega;
+    qm::launch_upw_backward(u, as_stream(stream));
+    qm::check(cudaGetLastError(), "weighted upsampling adjoint");
+  });
+}
+
+int qm_fuse_backward(const float *depth_in, const float *seeds_in, const int32_t *table,
+                     int width, int height, const float *grad_fused, float *grad_depth,
+                     void *stream)
+{
+  return guarded([&] {
+    check_stage_size(width, height);
+    require(depth_in && seeds_in && table && grad_fused && grad_depth, "NULL argument");
+    qm::DiffFuse f;
+    f.W = width;
+    f.H = height;
+    f.depth_in = depth_in;
+    f.seeds_in = reinterpret_cast<const float4 *>(seeds_in);
+    f.table = table;
+    f.g_fused = grad_fused;
+    f.g_depth = grad_depth;
+    qm::launch_fuse_bwd(f, as_stream(stream));
+    qm::check(cudaGetLastError(), "fusion adjoint");
   });
 }
 

@@ -498,10 +498,9 @@ __global__ void __launch_bounds__(kCellWarps * 32)
 }
 
 template <int D>
-void sweep_d(const Batch &B, int blocks, int level, int it, KParams kp, int arith,
-             cudaStream_t s)
+void sweep_d(const Batch &B, int blocks, int level, int parity, int first, KParams kp,
+             int arith, cudaStream_t s)
 {
-  const int parity = it & 1, first = it == 0 ? 1 : 0;
   if (arith == QM_ARITH_IEEE)
     k_bp_sweep<D, QM_ARITH_IEEE><<<blocks, kCellWarps * 32, 0, s>>>(B, level, parity, first, kp);
   else
@@ -550,18 +549,33 @@ void launch_msg_inherit(const Batch &B, int blocks, int level, int iters, int qt
 
 // A batch with mixed hypothesis counts launches one sweep per count present;
 // each launch skips the jobs of other counts.
-void launch_bp_sweep(const Batch &B, int blocks, int d, int level, int it, KParams kp, int arith,
-                     cudaStream_t s)
+namespace
+{
+void sweep_any(const Batch &B, int blocks, int d, int level, int parity, int first, KParams kp,
+               int arith, cudaStream_t s)
 {
   switch (d)
   {
-  case 32: sweep_d<32>(B, blocks, level, it, kp, arith, s); break;
-  case 48: sweep_d<48>(B, blocks, level, it, kp, arith, s); break;
-  case 64: sweep_d<64>(B, blocks, level, it, kp, arith, s); break;
-  case 96: sweep_d<96>(B, blocks, level, it, kp, arith, s); break;
-  case 128: sweep_d<128>(B, blocks, level, it, kp, arith, s); break;
+  case 32: sweep_d<32>(B, blocks, level, parity, first, kp, arith, s); break;
+  case 48: sweep_d<48>(B, blocks, level, parity, first, kp, arith, s); break;
+  case 64: sweep_d<64>(B, blocks, level, parity, first, kp, arith, s); break;
+  case 96: sweep_d<96>(B, blocks, level, parity, first, kp, arith, s); break;
+  case 128: sweep_d<128>(B, blocks, level, parity, first, kp, arith, s); break;
   default: break;
   }
+}
+} // namespace
+
+void launch_bp_sweep(const Batch &B, int blocks, int d, int level, int it, KParams kp, int arith,
+                     cudaStream_t s)
+{
+  sweep_any(B, blocks, d, level, it & 1, it == 0 ? 1 : 0, kp, arith, s);
+}
+
+void launch_bp_sweep_own(const Batch &B, int blocks, int d, int level, int parity, KParams kp,
+                         int arith, cudaStream_t s)
+{
+  sweep_any(B, blocks, d, level, parity, 0, kp, arith, s);
 }
 
 void launch_extract(const Batch &B, int blocks, int d,

@@ -45,6 +45,10 @@ void launch_msg_inherit(const Batch &B, int blocks, int level, int iters, int qt
 // half-sweep `it` (0-based) of level `level`
 void launch_bp_sweep(const Batch &B, int blocks, int d, int level, int it, KParams kp, int arith,
                      cudaStream_t s);
+// a half-sweep of colour `parity` that reads every incoming message from the
+// level's own buffers (all cells' starting messages already written)
+void launch_bp_sweep_own(const Batch &B, int blocks, int d, int level, int parity, KParams kp,
+                         int arith, cudaStream_t s);
 void launch_extract(const Batch &B, int blocks, int d, int arith, cudaStream_t s);
 void launch_row_solve(const Batch &B, int blocks, KParams kp, int arith, int max_w,
                       cudaStream_t s);
@@ -55,6 +59,72 @@ void launch_fuse_fill(const Batch &B, int blocks, cudaStream_t s);
 void launch_fuse_update(const Batch &B, int blocks, cudaStream_t s);
 // out[i] = seeds[i].w (the fused variance sigma^2), n pixels
 void launch_seed_variance(const float4 *seeds, float *out, long n, cudaStream_t s);
+
+// ---------------------------------------------------------------------------
+// Differentiable path (k_diff.cu).
+
+// One BP level of one keyframe for the soft readout and the BP adjoint.
+struct DiffBp
+{
+  int W, H, D;           // image and hypotheses
+  int w, h;              // cells of this level
+  int level, parity, qt_max;
+  const uint8_t *levels; // quadtree level map
+  const float *data;     // data term of this level
+  const float *S[4];     // messages read (a state snapshot, or the finals)
+  float *A[4];           // adjoint of the messages, by direction
+  float P1, P2;
+  double *gP;            // dL/dP1, dL/dP2 (accumulated)
+  float tau;             // readout temperature
+  double step, min_inv;  // hypothesis depths
+  float *sparse;         // readout output (W x H)
+  const float *g_sparse; // its adjoint
+};
+// soft readout at level-0 node cells: forward writes sparse; backward adds
+// the belief adjoint to A (the four incoming messages of every node cell)
+void launch_soft_readout(const DiffBp &a, int backward, cudaStream_t s);
+// adjoint of one half-sweep of colour a.parity: reads A at the updated cells
+// (then zeroes it) and adds to A at the messages they read (a.S is the state
+// the forward half-sweep read)
+void launch_bp_sweep_bwd(const DiffBp &a, cudaStream_t s);
+struct MsgPtrs
+{
+  float *m[4];
+};
+// parent.m[k] += sum of the (up to four) children's child.m[k], k = 0..3
+void launch_msg_downsample_add(const MsgPtrs &child, int cw, int ch, const MsgPtrs &parent,
+                               int pw, int ph, int D, cudaStream_t s);
+
+// Weighted upsampling of one image (FP64 line solves).
+struct DiffUp
+{
+  int W, H;
+  const uint8_t *img;
+  size_t pitch;
+  const float *omega;     // W x H edge-weight factors
+  double lam, sigma, row_closing, col_closing;
+  const float *sparse;    // input
+  float *dense;           // output
+  double *sd, *si;        // row-pass results (depth, indicator)
+  double *td, *ti;        // column-pass results
+  double *cp;             // Thomas scratch
+  double *ud, *ui;        // adjoint scratch
+  const float *g_dense;   // incoming adjoint
+  float *g_sparse, *g_omega;
+};
+void launch_upw_forward(const DiffUp &u, cudaStream_t s);
+void launch_upw_backward(const DiffUp &u, cudaStream_t s);
+
+struct DiffFuse
+{
+  int W, H;
+  const float *depth_in;  // upsampled depth before fusion
+  const float4 *seeds_in; // the transformed previous seeds
+  const int32_t *table;   // source seed per pixel (0 = none)
+  const float *g_fused;
+  float *g_depth;
+};
+void launch_fuse_bwd(const DiffFuse &f, cudaStream_t s);
 
 // supported hypothesis-count classes of the BP kernels
 bool bp_supported_d(int d);

@@ -110,6 +110,32 @@ def upsample(sparse, img, params: Params = Params(), dense=None):
     return out
 
 
+def bp_soft(cost, W, H, levels, params: Params, tau: float):
+    """FP64 hierarchical BP with the softened readout of the differentiable
+    path (disparity = sum softmax(-belief/tau) d).  Returns sparse (H, W)."""
+    cost = np.ascontiguousarray(cost, np.float64)
+    ch, cw, D = cost.shape
+    levels = np.ascontiguousarray(levels, np.int32)
+    labels = np.zeros((ch, cw), np.int32)
+    sp = np.zeros((H, W), np.float64)
+    pc = QmParamsC.from_params(params)
+    lib().orc_bp_soft_f64(_p(cost), W, H, _p(levels), ctypes.byref(pc), ctypes.c_double(tau),
+                          _p(labels), _p(sp))
+    return sp
+
+
+def upsample_w(sparse, img, params: Params, omega):
+    """FP64 upsampling with per-pixel edge-weight factors omega (H, W)."""
+    sparse = np.ascontiguousarray(sparse, np.float64)
+    img = np.ascontiguousarray(img, np.uint8)
+    omega = np.ascontiguousarray(omega, np.float64)
+    H, W = img.shape
+    out = np.zeros((H, W), np.float64)
+    pc = QmParamsC.from_params(params)
+    lib().orc_upsample_w_f64(_p(sparse), _p(img), W, H, ctypes.byref(pc), _p(omega), _p(out))
+    return out
+
+
 def upsample_weights(img, params: Params = Params()):
     img = np.ascontiguousarray(img, np.uint8)
     H, W = img.shape

@@ -395,7 +395,7 @@ void bp_half_sweep(Level<R> &L, int D, bool a_set, int lv, const int *qt, int W,
 // the final level-0 messages in the order up, down, left, right.
 template <typename R>
 void bp_extract(const R *cost, int W, int H, const int *qt, const orc_params &p, int *labels,
-                R *sparse, R *msg_out)
+                R *sparse, R *msg_out, double tau = 0.0)
 {
   const int D = p.num_hyp, NL = p.bp_levels;
   std::vector<Level<R>> lv(NL);
@@ -508,6 +508,22 @@ void bp_extract(const R *cost, int W, int H, const int *qt, const orc_params &p,
           if (std::isfinite(b_a))
             disparity = (R)best - b_a / (R)2;
         }
+        if (tau > 0.0)
+        {
+          // softened readout of the differentiable path (not in the
+          // reference): disparity = sum_d softmax(-b/tau)(d) * d
+          R bmin = b[0];
+          for (int d = 1; d < D; ++d)
+            bmin = std::min(bmin, b[d]);
+          R z = 0, s = 0;
+          for (int d = 0; d < D; ++d)
+          {
+            const R e = std::exp(-(b[d] - bmin) / (R)tau);
+            z += e;
+            s += e * (R)d;
+          }
+          disparity = s / z;
+        }
         const double dep = 1.0 / (p.inv_depth_step * (double)disparity + p.min_inv_depth);
         sparse[(size_t)(y * 4) * W + x * 4] = (R)dep;
       }
@@ -602,10 +618,23 @@ void thomas_line(int n, const R *w, size_t wstride, const R *rd, const R *ri, si
 // smooth_row only writes whole 16-sample chunks and smooth_col whole 8-row
 // chunks; the tails (W % 16, H % 8) keep whatever the output held.
 template <typename R>
-void upsample(const R *sparse, const uint8_t *img, int W, int H, const orc_params &p, R *dense)
+void upsample(const R *sparse, const uint8_t *img, int W, int H, const orc_params &p, R *dense,
+              const double *omega = nullptr)
 {
   std::vector<R> row_w((size_t)(W + 1) * H), col_w((size_t)W * (H + 1));
   upsample_weights(img, W, H, p, row_w.data(), col_w.data());
+  if (omega)
+  {
+    // per-pixel factors of the differentiable path (not in the reference):
+    // the edge between a pixel and its left / upper neighbour is scaled by
+    // the pixel's factor
+    for (int y = 0; y < H; ++y)
+      for (int x = 1; x < W; ++x)
+        row_w[(size_t)y * (W + 1) + x] *= (R)omega[(size_t)y * W + x];
+    for (int y = 1; y < H; ++y)
+      for (int x = 0; x < W; ++x)
+        col_w[(size_t)y * W + x] *= (R)omega[(size_t)y * W + x];
+  }
   const int wr = W / 16 * 16, hr = H / 8 * 8;
   std::vector<R> rd((size_t)W * H, (R)0), ri((size_t)W * H, (R)0);
   const R lambda = (R)p.up_lambda;
@@ -852,6 +881,19 @@ ORC_BP(orc_bp_f64, double)
   }
 ORC_UP(orc_upsample_f32, float)
 ORC_UP(orc_upsample_f64, double)
+
+// differentiable path: soft BP readout and weighted upsampling, FP64
+void orc_bp_soft_f64(const double *cost, int W, int H, const int *levels, const orc_params *p,
+                     double tau, int *labels, double *sparse)
+{
+  bp_extract<double>(cost, W, H, levels, *p, labels, sparse, nullptr, tau);
+}
+
+void orc_upsample_w_f64(const double *sparse, const uint8_t *img, int W, int H,
+                        const orc_params *p, const double *omega, double *dense)
+{
+  upsample<double>(sparse, img, W, H, *p, dense, omega);
+}
 
 void orc_upsample_weights_f32(const uint8_t *img, int W, int H, const orc_params *p,
                               float *row_w, float *col_w)
