@@ -405,6 +405,7 @@ def main():
         has = feed(i)
     assert all(has), "every stream must produce a depth map after %d frames" % WARM_FRAMES
     launches_per_step = batch.last_launches()
+    tune = batch.get_tune()  # launch shapes the autotuner chose on the first dense frame
     ext = torch.cuda.ExternalStream(batch.stream_ptr())
 
     # ---- device-resident batched steps (value)
@@ -521,6 +522,7 @@ def main():
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "streams_per_gpu": S, "global_batch": S * world,
                    "maps_per_step": S * world, "parallelism": "streams sharded per GPU",
+                   "launch_shapes": tune,
                    "l2": "inputs larger than L2: per-GPU working set %.1f GB per step"
                          % (S * 0.08)},
         "e2e": {"value": round(S * world / (e2e_ms * 1e-3), 2), "unit": "depth-maps/s",

@@ -177,6 +177,27 @@ int qm_batch_set_graphs(qm_batch *b, int enable);
  * it, so the range's half-sweeps hit L2.  0 = every level over all streams
  * at once (the default).  Results do not depend on it. */
 int qm_batch_set_group_bytes(qm_batch *b, size_t bytes);
+/* Launch shapes of the BP and line-solver kernels: warps per block of the
+ * BP half-sweeps and of the extraction (4, 8 or 16), rows per block of the
+ * row solve (1, 2 or 4) and columns per block of the column solve (2, 4 or
+ * 8).  The reference fixes its block shapes at compile time
+ * (bp_extract.cu, depth_upsample.cu launches); no counterpart. */
+typedef struct qm_tune
+{
+  int sweep_warps, extract_warps, row_warps, col_lines;
+} qm_tune;
+/* 1 = autotune (the default): every set of streams that runs together times
+ * three candidate shapes per kernel family on its first run (seven eager
+ * runs that change no result) and keeps the fastest; 0 = the fixed shapes
+ * (the defaults 8, 8, 2, 4 unless qm_batch_set_tune set others).  Results do
+ * not depend on the shapes. */
+int qm_batch_set_autotune(qm_batch *b, int enable);
+/* Fixes the shapes and turns autotune off.  QM_ERR_INVALID_ARG for a value
+ * outside the sets above or a line-solver block whose lines exceed the
+ * shared memory of a block for this batch's largest image. */
+int qm_batch_set_tune(qm_batch *b, const qm_tune *t);
+/* Shapes of the last dense-pipeline run (or profile). */
+int qm_batch_get_tune(qm_batch *b, qm_tune *t);
 /* Kernels launched by the last dense-pipeline run. */
 int qm_batch_last_launches(qm_batch *b, int *count);
 /* The cudaStream_t (as void*) every kernel of this batch is launched on;

@@ -83,6 +83,9 @@ _SIGS = {
     "qm_batch_device_depth": (_I, [_P, _I, ctypes.POINTER(_P)]),
     "qm_batch_set_graphs": (_I, [_P, _I]),
     "qm_batch_set_group_bytes": (_I, [_P, _S]),
+    "qm_batch_set_autotune": (_I, [_P, _I]),
+    "qm_batch_set_tune": (_I, [_P, ctypes.POINTER(_I)]),
+    "qm_batch_get_tune": (_I, [_P, ctypes.POINTER(_I)]),
     "qm_batch_last_launches": (_I, [_P, ctypes.POINTER(_I)]),
     "qm_batch_stream": (_I, [_P, ctypes.POINTER(_P)]),
     "qm_batch_profile": (_I, [_P, ctypes.POINTER(_F), ctypes.POINTER(_I)]),

@@ -630,6 +630,43 @@ int qm_batch_set_group_bytes(qm_batch *b, size_t bytes)
   });
 }
 
+int qm_batch_set_autotune(qm_batch *b, int enable)
+{
+  return guarded([&] {
+    require(b != nullptr, "NULL handle");
+    std::lock_guard<std::mutex> lock(b->set->mutex());
+    b->set->wait();
+    b->set->engine().set_autotune(enable != 0);
+  });
+}
+
+int qm_batch_set_tune(qm_batch *b, const qm_tune *t)
+{
+  return guarded([&] {
+    require(b && t, "NULL argument");
+    std::lock_guard<std::mutex> lock(b->set->mutex());
+    b->set->wait();
+    qm::Tune u;
+    u.sweep_warps = t->sweep_warps;
+    u.extract_warps = t->extract_warps;
+    u.row_warps = t->row_warps;
+    u.col_lines = t->col_lines;
+    b->set->engine().set_tune(u);
+  });
+}
+
+int qm_batch_get_tune(qm_batch *b, qm_tune *t)
+{
+  return guarded([&] {
+    require(b && t, "NULL argument");
+    const qm::Tune u = b->set->engine().last_tune();
+    t->sweep_warps = u.sweep_warps;
+    t->extract_warps = u.extract_warps;
+    t->row_warps = u.row_warps;
+    t->col_lines = u.col_lines;
+  });
+}
+
 int qm_batch_last_launches(qm_batch *b, int *count)
 {
   return guarded([&] {

@@ -50,7 +50,8 @@ struct Stages
   int count() const { return 7 + 3 * L; }
 };
 
-std::vector<int> stage_blocks(const Shape &s, const JobLayout &lay, const qm_params &p)
+std::vector<int> stage_blocks(const Shape &s, const JobLayout &lay, const qm_params &p,
+                              const Tune &tune)
 {
   const Stages st{p.bp_levels};
   std::vector<int> b(st.count(), 0);
@@ -63,12 +64,14 @@ std::vector<int> stage_blocks(const Shape &s, const JobLayout &lay, const qm_par
     b[st.pyr(l)] = cdiv((long)lay.lw[l] * lay.lh[l] * (D / 4), kFlatThreads);
   for (int l = 0; l < L; ++l)
     b[st.inherit(l)] = cdiv((long)lay.lw[l] * lay.lh[l] * (D / 4), kFlatThreads);
-  const int cpb = kCellWarps * bp_cells_per_warp(D); // BP cells per block
+  // BP cells per block of the half-sweeps and of the extraction
+  const int spb = tune.sweep_warps * bp_cells_per_warp(D);
+  const int epb = tune.extract_warps * bp_cells_per_warp(D);
   for (int l = 0; l < L; ++l)
-    b[st.sweep(l)] = cdiv((long)((lay.lw[l] + 1) / 2) * lay.lh[l], cpb);
-  b[st.extract()] = cdiv((long)lay.lw[0] * lay.lh[0], cpb);
-  b[st.row()] = cdiv(s.H, kRowWarps);
-  b[st.col()] = cdiv(s.W, kColLines);
+    b[st.sweep(l)] = cdiv((long)((lay.lw[l] + 1) / 2) * lay.lh[l], spb);
+  b[st.extract()] = cdiv((long)lay.lw[0] * lay.lh[0], epb);
+  b[st.row()] = cdiv(s.H, tune.row_warps);
+  b[st.col()] = cdiv(s.W, tune.col_lines);
   b[st.ftrans()] = b[st.ffill()] = b[st.fupd()] = cdiv((long)s.W * s.H, kFlatThreads);
   return b;
 }
@@ -83,6 +86,7 @@ struct StageTable
   std::vector<int> dvals;          // hypothesis counts present
   std::vector<size_t> level_bytes; // per job and BP level: data + messages
   int max_w = 0, max_h = 0;        // longest lines of the row / column solves
+  Tune tune;                       // launch shapes the blocks were counted for
 
   int begin(int stage, int j) const { return hprefix[(size_t)stage * (n + 1) + j]; }
   int blocks(int stage) const { return begin(stage, n); }
@@ -204,21 +208,25 @@ int enqueue_range(const Batch &B, const StageTable &T, const qm_params &p, size_
         if (grid > 0)
           for (int it = 0; it < p.bp_iters[l]; ++it)
             for (int d : T.dvals)
-              launch(kSweep, [&] { launch_bp_sweep(b, grid, d, l, it, kp, ar, s); });
+              launch(kSweep, [&] {
+                launch_bp_sweep(b, grid, d, l, it, kp, ar, s, T.tune.sweep_warps);
+              });
       }
       if (l == 0 && in(st.extract()))
       {
         const Batch b = at(st.extract(), j0, j1, grid);
         if (grid > 0)
           for (int d : T.dvals)
-            launch(kExtract, [&] { launch_extract(b, grid, d, ar, s); });
+            launch(kExtract, [&] { launch_extract(b, grid, d, ar, s, T.tune.extract_warps); });
       }
     }
   }
-  all(kRowSolve, st.row(),
-      [&](const Batch &b, int g) { launch_row_solve(b, g, kp, ar, T.max_w, s); });
-  all(kColSolve, st.col(),
-      [&](const Batch &b, int g) { launch_col_solve(b, g, kp, ar, T.max_h, s); });
+  all(kRowSolve, st.row(), [&](const Batch &b, int g) {
+    launch_row_solve(b, g, kp, ar, T.max_w, s, T.tune.row_warps);
+  });
+  all(kColSolve, st.col(), [&](const Batch &b, int g) {
+    launch_col_solve(b, g, kp, ar, T.max_h, s, T.tune.col_lines);
+  });
   all(kFuseTransform, st.ftrans(),
       [&](const Batch &b, int g) { launch_fuse_transform(b, g, ar, s); });
   all(kFuseFill, st.ffill(), [&](const Batch &b, int g) { launch_fuse_fill(b, g, s); });
@@ -404,22 +412,54 @@ JobDesc make_job_desc(const Shape &s, const qm_params &p, const JobBuffers &b, i
   return J;
 }
 
-struct Plan
+// Stage table of one job set under one set of launch shapes, with the device
+// copy of its block prefixes.
+struct TableBuf
 {
-  std::vector<int> active;
-  int *d_prefix = nullptr;
   StageTable table;
-  size_t group_bytes = 0;              // the job grouping the graphs were captured with
-  cudaGraphExec_t exec[2] = {nullptr, nullptr}; // by step parity
-  ~Plan()
+  int *d_prefix = nullptr;
+  TableBuf() = default;
+  TableBuf(const TableBuf &) = delete;
+  TableBuf &operator=(const TableBuf &) = delete;
+  ~TableBuf()
   {
-    for (auto e : exec)
-      if (e)
-        cudaGraphExecDestroy(e);
     if (d_prefix)
       cudaFree(d_prefix);
   }
 };
+
+struct Plan
+{
+  std::vector<int> active;
+  std::unique_ptr<TableBuf> tb;
+  bool tuned = false;                  // launch shapes settled (timed or fixed)
+  size_t group_bytes = 0;              // the job grouping the graphs were captured with
+  cudaGraphExec_t exec[2] = {nullptr, nullptr}; // by step parity
+  StageTable &table() { return tb->table; }
+  void drop_graphs()
+  {
+    for (auto &e : exec)
+      if (e)
+      {
+        cudaGraphExecDestroy(e);
+        e = nullptr;
+      }
+  }
+  ~Plan() { drop_graphs(); }
+};
+
+std::string validate(const Tune &t, int max_w, int max_h)
+{
+  auto one_of = [](int v, int a, int b, int c) { return v == a || v == b || v == c; };
+  if (!one_of(t.sweep_warps, 4, 8, 16) || !one_of(t.extract_warps, 4, 8, 16))
+    return "BP warps per block must be 4, 8 or 16";
+  if (!one_of(t.row_warps, 1, 2, 4) || !one_of(t.col_lines, 2, 4, 8))
+    return "row-solve rows per block must be 1, 2 or 4 and column-solve lines 2, 4 or 8";
+  if (row_solve_smem(max_w, t.row_warps) > (size_t)kMaxBlockSmem ||
+      col_solve_smem(max_h, t.col_lines) > (size_t)kMaxBlockSmem)
+    return "line-solver block exceeds the shared memory of a block at this image size";
+  return "";
+}
 
 Engine::Engine(int device, const qm_params &p, const std::vector<Shape> &shapes)
     : device_(device), params_(p), shapes_(shapes)
@@ -581,6 +621,37 @@ void Engine::reset_seeds(int j)
   seeds_cur_[j] = 0;
 }
 
+std::unique_ptr<TableBuf> Engine::build_table(const std::vector<int> &active, const Tune &tune)
+{
+  auto tb = std::make_unique<TableBuf>();
+  const int L = params_.bp_levels;
+  const int n = (int)active.size();
+  std::vector<std::vector<int>> per_job;
+  std::vector<int> ds;
+  StageTable &T = tb->table;
+  T.tune = tune;
+  for (int i = 0; i < n; ++i)
+  {
+    const int j = active[i];
+    ds.push_back(shapes_[j].D);
+    T.max_w = std::max(T.max_w, shapes_[j].W);
+    T.max_h = std::max(T.max_h, shapes_[j].H);
+    per_job.push_back(stage_blocks(shapes_[j], layouts_[j], params_, tune));
+    for (int l = 0; l < L; ++l)
+      T.level_bytes.push_back((size_t)5 * layouts_[j].lw[l] * layouts_[j].lh[l] * shapes_[j].D *
+                              sizeof(float));
+  }
+  T.add_jobs(per_job, ds);
+  const int ns = (int)T.uniform.size();
+  check(cudaMalloc((void **)&tb->d_prefix, sizeof(int) * T.hprefix.size()), "device allocation");
+  check(cudaMemcpy(tb->d_prefix, T.hprefix.data(), sizeof(int) * T.hprefix.size(),
+                   cudaMemcpyHostToDevice),
+        "plan upload");
+  for (int st = 0; st < ns; ++st)
+    T.prefix.push_back(tb->d_prefix + (size_t)st * (n + 1));
+  return tb;
+}
+
 Plan &Engine::plan_for(const std::vector<int> &active)
 {
   auto it = plans_.find(active);
@@ -588,43 +659,137 @@ Plan &Engine::plan_for(const std::vector<int> &active)
   {
     Plan &pl = *it->second;
     if (pl.group_bytes != group_bytes_)
-      for (auto &e : pl.exec)
-        if (e)
-        {
-          cudaGraphExecDestroy(e);
-          e = nullptr;
-        }
+      pl.drop_graphs();
     return pl;
   }
   auto pl = std::make_unique<Plan>();
   pl->active = active;
-  const int L = params_.bp_levels;
-  const int n = (int)active.size();
-  std::vector<std::vector<int>> per_job;
-  std::vector<int> ds;
-  StageTable &T = pl->table;
-  for (int i = 0; i < n; ++i)
+  int max_w = 0, max_h = 0;
+  for (int j : active)
   {
-    const int j = active[i];
-    ds.push_back(shapes_[j].D);
-    T.max_w = std::max(T.max_w, shapes_[j].W);
-    T.max_h = std::max(T.max_h, shapes_[j].H);
-    per_job.push_back(stage_blocks(shapes_[j], layouts_[j], params_));
-    for (int l = 0; l < L; ++l)
-      T.level_bytes.push_back((size_t)5 * layouts_[j].lw[l] * layouts_[j].lh[l] * shapes_[j].D *
-                              sizeof(float));
+    max_w = std::max(max_w, shapes_[j].W);
+    max_h = std::max(max_h, shapes_[j].H);
   }
-  T.add_jobs(per_job, ds);
-  const int ns = (int)T.uniform.size();
-  check(cudaMalloc((void **)&pl->d_prefix, sizeof(int) * T.hprefix.size()), "device allocation");
-  check(cudaMemcpy(pl->d_prefix, T.hprefix.data(), sizeof(int) * T.hprefix.size(),
-                   cudaMemcpyHostToDevice),
-        "plan upload");
-  for (int st = 0; st < ns; ++st)
-    T.prefix.push_back(pl->d_prefix + (size_t)st * (n + 1));
+  // a fixed shape that does not fit this set's lines falls back to the
+  // defaults (which fit every valid image size)
+  Tune t = fixed_tune_;
+  if (!validate(t, max_w, max_h).empty())
+    t = Tune{};
+  pl->tb = build_table(active, t);
+  pl->tuned = !autotune_;
   Plan &ref = *pl;
   plans_[active] = std::move(pl);
   return ref;
+}
+
+// Candidate c (0..2) of every launch-shape family; a line-solver candidate
+// that does not fit the set's longest line keeps the default.
+static Tune candidate(int c, int max_w, int max_h)
+{
+  static const int kWarps[3] = {4, 8, 16}, kRows[3] = {1, 2, 4}, kCols[3] = {2, 4, 8};
+  Tune t;
+  t.sweep_warps = t.extract_warps = kWarps[c];
+  if (row_solve_smem(max_w, kRows[c]) <= (size_t)kMaxBlockSmem)
+    t.row_warps = kRows[c];
+  if (col_solve_smem(max_h, kCols[c]) <= (size_t)kMaxBlockSmem)
+    t.col_lines = kCols[c];
+  return t;
+}
+
+void Engine::tune_plan(Plan &pl)
+{
+  // The candidates of the four families are timed side by side: run c uses
+  // candidate c of each, and every family keeps its fastest candidate by the
+  // summed device time of its launches.  Runs are eager, with an event pair
+  // around every launch; the first run warms the caches and is not counted,
+  // then each candidate runs twice and keeps its lower time.  A run writes
+  // the same buffers as the real run that follows (it reads the same seeds
+  // and inputs), so tuning changes no result.
+  const StageTable &T0 = pl.table();
+  std::unique_ptr<TableBuf> cand[3];
+  for (int c = 0; c < 3; ++c)
+    cand[c] = build_table(pl.active, candidate(c, T0.max_w, T0.max_h));
+  const Batch B = upload((int)pl.active.size(), stream_);
+  const Stages st{params_.bp_levels};
+  const int fam_kind[4] = {kSweep, kExtract, kRowSolve, kColSolve};
+  float best[3][4];
+  for (auto &r : best)
+    for (float &v : r)
+      v = INFINITY;
+  const int order[7] = {1, 0, 1, 2, 0, 1, 2};
+  for (int r = 0; r < 7; ++r)
+  {
+    const int c = order[r];
+    LaunchProfile prof;
+    float ms[kNumKinds] = {};
+    try
+    {
+      enqueue_range(B, cand[c]->table, params_, group_bytes_, 0, st.count() - 1, stream_, &prof);
+      check(cudaStreamSynchronize(stream_), "autotune run");
+    }
+    catch (...)
+    {
+      for (auto &m : prof.marks)
+      {
+        cudaEventDestroy(m.e0);
+        cudaEventDestroy(m.e1);
+      }
+      throw;
+    }
+    for (auto &m : prof.marks)
+    {
+      float t = 0.0f;
+      cudaEventElapsedTime(&t, m.e0, m.e1);
+      ms[m.kind] += t;
+      cudaEventDestroy(m.e0);
+      cudaEventDestroy(m.e1);
+    }
+    if (r > 0)
+      for (int f = 0; f < 4; ++f)
+        best[c][f] = std::min(best[c][f], ms[fam_kind[f]]);
+  }
+  int pick[4];
+  for (int f = 0; f < 4; ++f)
+  {
+    pick[f] = 1;
+    for (int c = 0; c < 3; ++c)
+      if (best[c][f] < best[pick[f]][f])
+        pick[f] = c;
+  }
+  Tune t;
+  t.sweep_warps = cand[pick[0]]->table.tune.sweep_warps;
+  t.extract_warps = cand[pick[1]]->table.tune.extract_warps;
+  t.row_warps = cand[pick[2]]->table.tune.row_warps;
+  t.col_lines = cand[pick[3]]->table.tune.col_lines;
+  pl.drop_graphs();
+  pl.tb = build_table(pl.active, t);
+  pl.tuned = true;
+}
+
+void Engine::set_autotune(bool on)
+{
+  check(cudaSetDevice(device_), "cudaSetDevice");
+  check(cudaStreamSynchronize(stream_), "autotune switch");
+  autotune_ = on;
+  plans_.clear();
+}
+
+void Engine::set_tune(const Tune &t)
+{
+  int max_w = 0, max_h = 0;
+  for (const auto &s : shapes_)
+  {
+    max_w = std::max(max_w, s.W);
+    max_h = std::max(max_h, s.H);
+  }
+  const std::string err = validate(t, max_w, max_h);
+  if (!err.empty())
+    throw CudaError{QM_ERR_INVALID_ARG, err};
+  check(cudaSetDevice(device_), "cudaSetDevice");
+  check(cudaStreamSynchronize(stream_), "launch-shape switch");
+  fixed_tune_ = t;
+  autotune_ = false;
+  plans_.clear();
 }
 
 void Engine::pack(const std::vector<int> &active)
@@ -669,7 +834,7 @@ int Engine::enqueue(Plan &pl, cudaStream_t s)
   const Batch B = upload((int)pl.active.size(), s);
   const Stages st{params_.bp_levels};
   pl.group_bytes = group_bytes_;
-  return enqueue_range(B, pl.table, params_, group_bytes_, 0, st.count() - 1, s);
+  return enqueue_range(B, pl.table(), params_, group_bytes_, 0, st.count() - 1, s);
 }
 
 void Engine::run(const std::vector<int> &active)
@@ -685,6 +850,9 @@ void Engine::launch(const std::vector<int> &active)
   check(cudaSetDevice(device_), "cudaSetDevice");
   Plan &pl = plan_for(active);
   pack(active);
+  if (!pl.tuned)
+    tune_plan(pl);
+  last_tune_ = pl.table().tune;
   if (graphs_)
   {
     // one graph per parity: its memcpy nodes read that parity's pinned
@@ -738,12 +906,15 @@ void Engine::profile(const std::vector<int> &active, float *ms, int *launches)
   check(cudaSetDevice(device_), "cudaSetDevice");
   Plan &pl = plan_for(active);
   pack(active);
+  if (!pl.tuned)
+    tune_plan(pl);
+  last_tune_ = pl.table().tune;
   const Batch B = upload((int)pl.active.size(), stream_);
   const Stages st{params_.bp_levels};
   LaunchProfile prof;
   try
   {
-    enqueue_range(B, pl.table, params_, group_bytes_, 0, st.count() - 1, stream_, &prof);
+    enqueue_range(B, pl.table(), params_, group_bytes_, 0, st.count() - 1, stream_, &prof);
     check(cudaStreamSynchronize(stream_), "profile run");
   }
   catch (...)
@@ -794,7 +965,7 @@ int run_range(const Batch &B, const Shape &s, const qm_params &p, int first, int
 {
   const JobLayout lay = JobLayout::make(s, p.bp_levels);
   StageTable T;
-  T.add_jobs({stage_blocks(s, lay, p)}, {s.D});
+  T.add_jobs({stage_blocks(s, lay, p, T.tune)}, {s.D});
   T.max_w = s.W;
   T.max_h = s.H;
   return enqueue_range(B, T, p, 0, first, last, stream);

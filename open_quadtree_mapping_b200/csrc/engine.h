@@ -120,6 +120,10 @@ int dedupe_slots(int F, const uint8_t *const *ptrs, const float *T, const uint8_
 // Stage plan of one active job set: block prefix per stage, in one device
 // buffer, plus the captured graph.
 struct Plan;
+struct TableBuf;
+
+// Validates launch shapes for lines up to max_w / max_h samples.
+std::string validate(const Tune &t, int max_w, int max_h);
 
 class Engine
 {
@@ -162,6 +166,15 @@ public:
   void set_group_bytes(size_t bytes) { group_bytes_ = bytes; }
   size_t group_bytes() const { return group_bytes_; }
   int last_launches() const { return last_launches_; }
+  // Launch shapes of the BP and line-solver kernels.  With autotune on (the
+  // default) each active job set times three candidates per kernel family
+  // on its first run and keeps the fastest; set_tune fixes the shapes for
+  // every set (autotune off).  Results do not depend on the shapes.
+  void set_autotune(bool on);
+  bool autotune() const { return autotune_; }
+  void set_tune(const Tune &t);
+  // shapes of the last launched or profiled set
+  Tune last_tune() const { return last_tune_; }
   // Events bracketing the device work of the last run (for timing).
   float last_run_ms() const;
   // Runs the pipeline once with eager launches, each bracketed by events;
@@ -171,6 +184,8 @@ public:
 
 private:
   Plan &plan_for(const std::vector<int> &active);
+  std::unique_ptr<TableBuf> build_table(const std::vector<int> &active, const Tune &tune);
+  void tune_plan(Plan &pl);
   // packs the descriptors of `active` into the pinned run array
   void pack(const std::vector<int> &active);
   // enqueues the descriptor and slot-table uploads; returns the batch
@@ -203,6 +218,8 @@ private:
   int parity_ = 0;
   size_t group_bytes_ = kDefaultGroupBytes;
   int last_launches_ = 0;
+  bool autotune_ = true;
+  Tune fixed_tune_, last_tune_;
   std::map<std::vector<int>, std::unique_ptr<Plan>> plans_;
 };
 

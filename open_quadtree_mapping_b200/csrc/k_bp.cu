@@ -265,7 +265,7 @@ __global__ void __launch_bounds__(kFlatThreads)
 // colour.  Groups whose cell is skipped or out of range still take part in
 // the warp's shuffles (full masks) with zero inputs and store nothing.
 template <int D, int ARITH>
-__global__ void __launch_bounds__(kCellWarps * 32, 7)
+__global__ void __launch_bounds__(kMaxCellWarps * 32, 4)
     k_bp_sweep(const __grid_constant__ Batch B, int level, int parity, int first, KParams kp)
 {
   using HL = HypLayout<D>;
@@ -277,7 +277,7 @@ __global__ void __launch_bounds__(kCellWarps * 32, 7)
   const LevelDesc &L = J.lv[level];
   const int w = L.w, h = L.h, hw = (w + 1) / 2;
   const int lane = threadIdx.x & 31, gl = lane & (LPC - 1);
-  const int item0 = (lb * kCellWarps + (threadIdx.x >> 5)) * G;
+  const int item0 = (lb * (int)(blockDim.x >> 5) + (threadIdx.x >> 5)) * G;
   if (item0 >= hw * h)
     return; // the whole warp
   const int item = item0 + lane / LPC;
@@ -393,7 +393,7 @@ __global__ void __launch_bounds__(kCellWarps * 32, 7)
 // ------------------------------------------------------------- extract
 // depth_extract (bpextract.cu:314-372), one lane group per level-0 cell.
 template <int D, int ARITH>
-__global__ void __launch_bounds__(kCellWarps * 32)
+__global__ void __launch_bounds__(kMaxCellWarps * 32)
     k_extract(const __grid_constant__ Batch B)
 {
   using HL = HypLayout<D>;
@@ -405,7 +405,7 @@ __global__ void __launch_bounds__(kCellWarps * 32)
   const LevelDesc &L = J.lv[0];
   const int w = L.w, h = L.h;
   const int lane = threadIdx.x & 31, gl = lane & (LPC - 1);
-  const int cell0 = (lb * kCellWarps + (threadIdx.x >> 5)) * G;
+  const int cell0 = (lb * (int)(blockDim.x >> 5) + (threadIdx.x >> 5)) * G;
   if (cell0 >= w * h)
     return; // the whole warp
   const int cell = cell0 + lane / LPC;
@@ -499,23 +499,21 @@ __global__ void __launch_bounds__(kCellWarps * 32)
 
 template <int D>
 void sweep_d(const Batch &B, int blocks, int level, int parity, int first, KParams kp,
-             int arith, cudaStream_t s)
+             int arith, int warps, cudaStream_t s)
 {
   if (arith == QM_ARITH_IEEE)
-    k_bp_sweep<D, QM_ARITH_IEEE><<<blocks, kCellWarps * 32, 0, s>>>(B, level, parity, first, kp);
+    k_bp_sweep<D, QM_ARITH_IEEE><<<blocks, warps * 32, 0, s>>>(B, level, parity, first, kp);
   else
-    k_bp_sweep<D, QM_ARITH_REFERENCE><<<blocks, kCellWarps * 32, 0, s>>>(B, level, parity, first,
-                                                                         kp);
+    k_bp_sweep<D, QM_ARITH_REFERENCE><<<blocks, warps * 32, 0, s>>>(B, level, parity, first, kp);
 }
 
 template <int D>
-void extract_d(const Batch &B, int blocks, int arith,
-               cudaStream_t s)
+void extract_d(const Batch &B, int blocks, int arith, int warps, cudaStream_t s)
 {
   if (arith == QM_ARITH_IEEE)
-    k_extract<D, QM_ARITH_IEEE><<<blocks, kCellWarps * 32, 0, s>>>(B);
+    k_extract<D, QM_ARITH_IEEE><<<blocks, warps * 32, 0, s>>>(B);
   else
-    k_extract<D, QM_ARITH_REFERENCE><<<blocks, kCellWarps * 32, 0, s>>>(B);
+    k_extract<D, QM_ARITH_REFERENCE><<<blocks, warps * 32, 0, s>>>(B);
 }
 
 } // namespace
@@ -552,42 +550,41 @@ void launch_msg_inherit(const Batch &B, int blocks, int level, int iters, int qt
 namespace
 {
 void sweep_any(const Batch &B, int blocks, int d, int level, int parity, int first, KParams kp,
-               int arith, cudaStream_t s)
+               int arith, int warps, cudaStream_t s)
 {
   switch (d)
   {
-  case 32: sweep_d<32>(B, blocks, level, parity, first, kp, arith, s); break;
-  case 48: sweep_d<48>(B, blocks, level, parity, first, kp, arith, s); break;
-  case 64: sweep_d<64>(B, blocks, level, parity, first, kp, arith, s); break;
-  case 96: sweep_d<96>(B, blocks, level, parity, first, kp, arith, s); break;
-  case 128: sweep_d<128>(B, blocks, level, parity, first, kp, arith, s); break;
+  case 32: sweep_d<32>(B, blocks, level, parity, first, kp, arith, warps, s); break;
+  case 48: sweep_d<48>(B, blocks, level, parity, first, kp, arith, warps, s); break;
+  case 64: sweep_d<64>(B, blocks, level, parity, first, kp, arith, warps, s); break;
+  case 96: sweep_d<96>(B, blocks, level, parity, first, kp, arith, warps, s); break;
+  case 128: sweep_d<128>(B, blocks, level, parity, first, kp, arith, warps, s); break;
   default: break;
   }
 }
 } // namespace
 
 void launch_bp_sweep(const Batch &B, int blocks, int d, int level, int it, KParams kp, int arith,
-                     cudaStream_t s)
+                     cudaStream_t s, int warps)
 {
-  sweep_any(B, blocks, d, level, it & 1, it == 0 ? 1 : 0, kp, arith, s);
+  sweep_any(B, blocks, d, level, it & 1, it == 0 ? 1 : 0, kp, arith, warps, s);
 }
 
 void launch_bp_sweep_own(const Batch &B, int blocks, int d, int level, int parity, KParams kp,
-                         int arith, cudaStream_t s)
+                         int arith, cudaStream_t s, int warps)
 {
-  sweep_any(B, blocks, d, level, parity, 0, kp, arith, s);
+  sweep_any(B, blocks, d, level, parity, 0, kp, arith, warps, s);
 }
 
-void launch_extract(const Batch &B, int blocks, int d,
-                    int arith, cudaStream_t s)
+void launch_extract(const Batch &B, int blocks, int d, int arith, cudaStream_t s, int warps)
 {
   switch (d)
   {
-  case 32: extract_d<32>(B, blocks, arith, s); break;
-  case 48: extract_d<48>(B, blocks, arith, s); break;
-  case 64: extract_d<64>(B, blocks, arith, s); break;
-  case 96: extract_d<96>(B, blocks, arith, s); break;
-  case 128: extract_d<128>(B, blocks, arith, s); break;
+  case 32: extract_d<32>(B, blocks, arith, warps, s); break;
+  case 48: extract_d<48>(B, blocks, arith, warps, s); break;
+  case 64: extract_d<64>(B, blocks, arith, warps, s); break;
+  case 96: extract_d<96>(B, blocks, arith, warps, s); break;
+  case 128: extract_d<128>(B, blocks, arith, warps, s); break;
   default: break;
   }
 }

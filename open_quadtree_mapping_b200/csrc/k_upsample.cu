@@ -29,9 +29,10 @@
 // warp keeps its line in shared memory in a skewed layout (segment j of lane
 // l at l*mp + j, mp odd) so that lane-parallel accesses are conflict-free.
 //
-// Row pass: a block holds kRowWarps rows; loads and stores are coalesced
-// along the row.  Column pass: a block holds a stripe of kColLines columns,
-// loaded and stored cooperatively row by row.
+// Row pass: a block holds one row per warp (blockDim.x / 32 rows, chosen at
+// launch); loads and stores are coalesced along the row.  Column pass: a block
+// holds a stripe of one column per warp, loaded and stored cooperatively row
+// by row.
 // Bytes per pixel: row pass 1 (image) + 4 (sparse) read, 8 written; column
 // pass 1 + 8 read, 4 written.
 #include "launch.h"
@@ -242,7 +243,7 @@ __device__ void solve_line(const LineBuf &b, double lam)
 }
 
 template <class A>
-__global__ void __launch_bounds__(kRowWarps * 32)
+__global__ void __launch_bounds__(kMaxRowWarps * 32)
     k_row_solve(const __grid_constant__ Batch B, KParams kp, int max_n)
 {
   extern __shared__ float smem[];
@@ -250,7 +251,7 @@ __global__ void __launch_bounds__(kRowWarps * 32)
   const JobDesc &J = job_of(B, lb);
   const int W = J.W, H = J.H;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int y = lb * kRowWarps + warp;
+  const int y = lb * (int)(blockDim.x >> 5) + warp;
   if (y >= H)
     return;
   const int n = W / 16 * 16;
@@ -280,7 +281,7 @@ __global__ void __launch_bounds__(kRowWarps * 32)
 }
 
 template <class A>
-__global__ void __launch_bounds__(kColLines * 32)
+__global__ void __launch_bounds__(kMaxColLines * 32)
     k_col_solve(const __grid_constant__ Batch B, KParams kp, int max_n)
 {
   extern __shared__ float smem[];
@@ -288,13 +289,14 @@ __global__ void __launch_bounds__(kColLines * 32)
   const JobDesc &J = job_of(B, lb);
   const int W = J.W, H = J.H;
   const int warp = threadIdx.x >> 5;
-  const int x0 = lb * kColLines;
+  const int lines = blockDim.x >> 5;
+  const int x0 = lb * lines;
   const int n = H / 8 * 8;
   const int per_line = kArrays * line_floats(max_n);
   // cooperative stripe load: row k, column x0 + c
-  for (int t = threadIdx.x; t < n * kColLines; t += blockDim.x)
+  for (int t = threadIdx.x; t < n * lines; t += blockDim.x)
   {
-    const int k = t / kColLines, c = t - k * kColLines;
+    const int k = t / lines, c = t - k * lines;
     const int x = x0 + c;
     if (x >= W)
       continue;
@@ -316,9 +318,9 @@ __global__ void __launch_bounds__(kColLines * 32)
   if (x0 + warp < W)
     solve_line(line_buf(smem + warp * per_line, n), kp.up_lambda);
   __syncthreads();
-  for (int t = threadIdx.x; t < n * kColLines; t += blockDim.x)
+  for (int t = threadIdx.x; t < n * lines; t += blockDim.x)
   {
-    const int k = t / kColLines, c = t - k * kColLines;
+    const int k = t / lines, c = t - k * lines;
     const int x = x0 + c;
     if (x >= W)
       continue;
@@ -330,12 +332,18 @@ __global__ void __launch_bounds__(kColLines * 32)
 
 } // namespace
 
-size_t row_solve_smem(int max_w) { return sizeof(float) * kRowWarps * kArrays * line_floats(max_w); }
-size_t col_solve_smem(int max_h) { return sizeof(float) * kColLines * kArrays * line_floats(max_h); }
+size_t row_solve_smem(int max_w, int rows)
+{
+  return sizeof(float) * rows * kArrays * line_floats(max_w);
+}
+size_t col_solve_smem(int max_h, int lines)
+{
+  return sizeof(float) * lines * kArrays * line_floats(max_h);
+}
 
 void prepare_upsample_kernels()
 {
-  const int mx = 227 * 1024;
+  const int mx = kMaxBlockSmem;
   cudaFuncSetAttribute(k_row_solve<ArithRef>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
   cudaFuncSetAttribute(k_row_solve<ArithIeee>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
   cudaFuncSetAttribute(k_col_solve<ArithRef>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
@@ -367,25 +375,25 @@ void prepare_once_for_current_device()
 } // namespace
 
 void launch_row_solve(const Batch &B, int blocks, KParams kp, int arith, int max_w,
-                      cudaStream_t s)
+                      cudaStream_t s, int rows)
 {
   prepare_once_for_current_device();
-  const size_t sm = row_solve_smem(max_w);
+  const size_t sm = row_solve_smem(max_w, rows);
   if (arith == QM_ARITH_IEEE)
-    k_row_solve<ArithIeee><<<blocks, kRowWarps * 32, sm, s>>>(B, kp, max_w);
+    k_row_solve<ArithIeee><<<blocks, rows * 32, sm, s>>>(B, kp, max_w);
   else
-    k_row_solve<ArithRef><<<blocks, kRowWarps * 32, sm, s>>>(B, kp, max_w);
+    k_row_solve<ArithRef><<<blocks, rows * 32, sm, s>>>(B, kp, max_w);
 }
 
 void launch_col_solve(const Batch &B, int blocks, KParams kp, int arith, int max_h,
-                      cudaStream_t s)
+                      cudaStream_t s, int lines)
 {
   prepare_once_for_current_device();
-  const size_t sm = col_solve_smem(max_h);
+  const size_t sm = col_solve_smem(max_h, lines);
   if (arith == QM_ARITH_IEEE)
-    k_col_solve<ArithIeee><<<blocks, kColLines * 32, sm, s>>>(B, kp, max_h);
+    k_col_solve<ArithIeee><<<blocks, lines * 32, sm, s>>>(B, kp, max_h);
   else
-    k_col_solve<ArithRef><<<blocks, kColLines * 32, sm, s>>>(B, kp, max_h);
+    k_col_solve<ArithRef><<<blocks, lines * 32, sm, s>>>(B, kp, max_h);
 }
 
 } // namespace qm

@@ -12,17 +12,34 @@ namespace qm
 
 // threads per block of the flat per-element kernels
 constexpr int kFlatThreads = 256;
-// warps per block of the warp-per-cell kernels (BP sweep, extraction)
+// warps per block of the warp-per-cell kernels (BP sweep, extraction): the
+// default and the largest the kernels are compiled for (the autotuner picks
+// among 4, 8 and 16)
 constexpr int kCellWarps = 8;
+constexpr int kMaxCellWarps = 16;
 // line solvers: one warp per line; rows per block of the row pass and
-// columns per block (stripe width) of the column pass
+// columns per block (stripe width) of the column pass: defaults and maxima
 constexpr int kRowWarps = 2;
 constexpr int kColLines = 4;
+constexpr int kMaxRowWarps = 4;
+constexpr int kMaxColLines = 8;
 // longest lines the solvers' shared memory holds
 constexpr int kMaxRowLen = 4096;
 constexpr int kMaxColLen = 2048;
-size_t row_solve_smem(int max_w);
-size_t col_solve_smem(int max_h);
+size_t row_solve_smem(int max_w, int rows = kRowWarps);
+size_t col_solve_smem(int max_h, int lines = kColLines);
+
+// shared memory one block may take
+constexpr int kMaxBlockSmem = 227 * 1024;
+
+// Launch shapes of one active job set (chosen by the engine's autotuner).
+struct Tune
+{
+  int sweep_warps = kCellWarps;   // warps per block of the BP half-sweeps
+  int extract_warps = kCellWarps; // warps per block of the extraction
+  int row_warps = kRowWarps;      // rows per block of the row solve
+  int col_lines = kColLines;      // columns per block of the column solve
+};
 void prepare_upsample_kernels();
 
 // blocks of the quadtree launch for one W x H image
@@ -42,18 +59,19 @@ void launch_pyramid(const Batch &B, int blocks, int level, cudaStream_t s);
 // (cells the quadtree test skips; all unswept cells when iters < 2)
 void launch_msg_inherit(const Batch &B, int blocks, int level, int iters, int qt_max,
                         cudaStream_t s);
-// half-sweep `it` (0-based) of level `level`
+// half-sweep `it` (0-based) of level `level`; `warps` per block
 void launch_bp_sweep(const Batch &B, int blocks, int d, int level, int it, KParams kp, int arith,
-                     cudaStream_t s);
+                     cudaStream_t s, int warps = kCellWarps);
 // a half-sweep of colour `parity` that reads every incoming message from the
 // level's own buffers (all cells' starting messages already written)
 void launch_bp_sweep_own(const Batch &B, int blocks, int d, int level, int parity, KParams kp,
-                         int arith, cudaStream_t s);
-void launch_extract(const Batch &B, int blocks, int d, int arith, cudaStream_t s);
+                         int arith, cudaStream_t s, int warps = kCellWarps);
+void launch_extract(const Batch &B, int blocks, int d, int arith, cudaStream_t s,
+                    int warps = kCellWarps);
 void launch_row_solve(const Batch &B, int blocks, KParams kp, int arith, int max_w,
-                      cudaStream_t s);
+                      cudaStream_t s, int rows = kRowWarps);
 void launch_col_solve(const Batch &B, int blocks, KParams kp, int arith, int max_h,
-                      cudaStream_t s);
+                      cudaStream_t s, int lines = kColLines);
 void launch_fuse_transform(const Batch &B, int blocks, int arith, cudaStream_t s);
 void launch_fuse_fill(const Batch &B, int blocks, cudaStream_t s);
 void launch_fuse_update(const Batch &B, int blocks, cudaStream_t s);

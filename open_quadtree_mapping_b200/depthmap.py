@@ -261,6 +261,23 @@ class BatchDepthmap:
         """L2 budget of a BP job range (0 = all streams at once)."""
         _lib.check(_lib.lib().qm_batch_set_group_bytes(self._h, int(nbytes)))
 
+    TUNE_FIELDS = ("sweep_warps", "extract_warps", "row_warps", "col_lines")
+
+    def set_autotune(self, on: bool) -> None:
+        """Time candidate launch shapes per active stream set (default on)."""
+        _lib.check(_lib.lib().qm_batch_set_autotune(self._h, 1 if on else 0))
+
+    def set_tune(self, sweep_warps=8, extract_warps=8, row_warps=2, col_lines=4) -> None:
+        """Fix the launch shapes (turns autotune off)."""
+        t = (ctypes.c_int * 4)(sweep_warps, extract_warps, row_warps, col_lines)
+        _lib.check(_lib.lib().qm_batch_set_tune(self._h, t))
+
+    def get_tune(self) -> dict:
+        """Launch shapes of the last run."""
+        t = (ctypes.c_int * 4)()
+        _lib.check(_lib.lib().qm_batch_get_tune(self._h, t))
+        return dict(zip(self.TUNE_FIELDS, list(t)))
+
     def last_launches(self) -> int:
         c = ctypes.c_int()
         _lib.check(_lib.lib().qm_batch_last_launches(self._h, ctypes.byref(c)))
