@@ -117,6 +117,14 @@ int qm_depthmap_get_variance(qm_depthmap *h, float *out, size_t stride);
 int qm_depthmap_get_reference(qm_depthmap *h, uint8_t *out, size_t stride);
 /* getT_world_ref (depthmap.h:74). */
 int qm_depthmap_get_T_world_ref(qm_depthmap *h, float T[12]);
+/* Publisher::publishPointCloud (publisher.cpp:129-166) on the last result:
+ * every pixel of the fused depth not below 0.1 gives the point
+ * T_world_ref * (normalize(((x-cx)/fx, (y-cy)/fy, 1)) * depth) with the
+ * reference image's intensity, in row-major pixel order, bit-identical to the
+ * reference's host loop.  points: host, 4 floats (x, y, z, intensity) per
+ * point; at most `capacity` points are written (width*height always
+ * suffices); *count receives the number of points of the cloud. */
+int qm_depthmap_get_point_cloud(qm_depthmap *h, float *points, size_t capacity, int *count);
 /* getFx/Fy/Cx/Cy/Width/Height (depthmap.h:53-72). */
 int qm_depthmap_get_camera(qm_depthmap *h, qm_camera *cam, int *width, int *height);
 
@@ -160,6 +168,9 @@ int qm_batch_wait(qm_batch *b);
 int qm_batch_get_depth(qm_batch *b, int stream, float *out, size_t stride);
 int qm_batch_get_debug(qm_batch *b, int stream, float *out, size_t stride);
 int qm_batch_get_variance(qm_batch *b, int stream, float *out, size_t stride);
+/* qm_depthmap_get_point_cloud for stream i of the batch. */
+int qm_batch_get_point_cloud(qm_batch *b, int stream, float *points, size_t capacity,
+                             int *count);
 /* Fused depth of n streams in one call: streams[k] is written to outs[k]
  * (row pitch strides[k] elements); the downloads are issued together and
  * waited for once. */
@@ -287,6 +298,18 @@ int qm_fuse_workspace_size(int width, int height, size_t *bytes);
 int qm_fuse(float *depth, float *seeds_in, float *seeds_out, const float T_income_last[12],
             const qm_camera *cam, int width, int height, const qm_params *p, int32_t *table,
             void *workspace, size_t workspace_bytes, void *stream);
+
+/* The point cloud of qm_depthmap_get_point_cloud for any depth map on the
+ * device: depth (f32, row stride depth_stride floats), ref (u8, row pitch
+ * ref_pitch bytes), T_world_ref HOST 12 floats.  points: device, 4 floats
+ * per point, room for width*height points; count: device int, written when
+ * the work on `stream` completes.  Workspace from
+ * qm_point_cloud_workspace_size. */
+int qm_point_cloud_workspace_size(int width, int height, size_t *bytes);
+int qm_point_cloud(const float *depth, size_t depth_stride, const uint8_t *ref, size_t ref_pitch,
+                   int width, int height, const qm_camera *cam, const float T_world_ref[12],
+                   float *points, int *count, void *workspace, size_t workspace_bytes,
+                   void *stream);
 
 /* ------------------------------------------------- differentiable path ----
  * For fitting the BP penalties (P1, P2) and per-pixel upsampling weight

@@ -116,6 +116,16 @@ public:
   {
     qm_check(qm_depthmap_get_reference(h_, out, stride));
   }
+  // The cloud Publisher::publishPointCloud builds from the last result
+  // (publisher.cpp:129-166): (x, y, z, intensity) per point, world frame.
+  std::vector<float> getPointCloud() const
+  {
+    std::vector<float> pts((size_t)width_ * height_ * 4);
+    int n = 0;
+    qm_check(qm_depthmap_get_point_cloud(h_, pts.data(), (size_t)width_ * height_, &n));
+    pts.resize((size_t)n * 4);
+    return pts;
+  }
   void getT_world_ref(float T[12]) const
   {
     for (int i = 0; i < 12; ++i)

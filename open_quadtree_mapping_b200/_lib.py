@@ -66,6 +66,7 @@ _SIGS = {
     "qm_depthmap_get_debug": (_I, [_P, _P, _S]),
     "qm_depthmap_get_reference": (_I, [_P, _P, _S]),
     "qm_depthmap_get_variance": (_I, [_P, _P, _S]),
+    "qm_depthmap_get_point_cloud": (_I, [_P, _P, _S, ctypes.POINTER(_I)]),
     "qm_depthmap_get_T_world_ref": (_I, [_P, _P]),
     "qm_depthmap_get_camera": (_I, [_P, ctypes.POINTER(QmCamera), ctypes.POINTER(_I),
                                     ctypes.POINTER(_I)]),
@@ -78,6 +79,7 @@ _SIGS = {
     "qm_batch_wait": (_I, [_P]),
     "qm_batch_get_debug": (_I, [_P, _I, _P, _S]),
     "qm_batch_get_variance": (_I, [_P, _I, _P, _S]),
+    "qm_batch_get_point_cloud": (_I, [_P, _I, _P, _S, ctypes.POINTER(_I)]),
     "qm_batch_get_depths": (_I, [_P, _I, _P, _P, _P]),
     "qm_batch_run_resident": (_I, [_P]),
     "qm_batch_device_depth": (_I, [_P, _I, ctypes.POINTER(_P)]),
@@ -98,6 +100,9 @@ _SIGS = {
     "qm_upsample": (_I, [_P, _P, _S, _I, _I, ctypes.POINTER(QmParamsC), _P, _P, _S, _P]),
     "qm_upsample_noalloc": (_I, [_P, _P, _S, _I, _I, ctypes.POINTER(QmParamsC), _P, _P]),
     "qm_fuse_workspace_size": (_I, [_I, _I, ctypes.POINTER(_S)]),
+    "qm_point_cloud_workspace_size": (_I, [_I, _I, ctypes.POINTER(_S)]),
+    "qm_point_cloud": (_I, [_P, _S, _P, _S, _I, _I, ctypes.POINTER(QmCamera), _P, _P, _P, _P,
+                            _S, _P]),
     "qm_fuse": (_I, [_P, _P, _P, _P, ctypes.POINTER(QmCamera), _I, _I,
                      ctypes.POINTER(QmParamsC), _P, _P, _S, _P]),
     "qm_bp_soft_workspace_size": (_I, [_I, _I, ctypes.POINTER(QmParamsC), ctypes.POINTER(_S)]),

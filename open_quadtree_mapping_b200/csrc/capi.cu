@@ -477,6 +477,15 @@ int qm_depthmap_get_T_world_ref(qm_depthmap *h, float T[12])
   });
 }
 
+int qm_depthmap_get_point_cloud(qm_depthmap *h, float *points, size_t capacity, int *count)
+{
+  return guarded([&] {
+    require(h && count && (points || capacity == 0), "bad argument");
+    std::lock_guard<std::mutex> lock(h->set->mutex());
+    *count = h->set->get_point_cloud(0, points, capacity);
+  });
+}
+
 int qm_depthmap_get_camera(qm_depthmap *h, qm_camera *cam, int *width, int *height)
 {
   return guarded([&] {
@@ -591,6 +600,17 @@ int qm_batch_get_variance(qm_batch *b, int stream, float *out, size_t stride)
             "bad argument");
     std::lock_guard<std::mutex> lock(b->set->mutex());
     b->set->get_variance(stream, out, stride);
+  });
+}
+
+int qm_batch_get_point_cloud(qm_batch *b, int stream, float *points, size_t capacity,
+                             int *count)
+{
+  return guarded([&] {
+    require(b && count && (points || capacity == 0) && stream >= 0 && stream < b->set->size(),
+            "bad argument");
+    std::lock_guard<std::mutex> lock(b->set->mutex());
+    *count = b->set->get_point_cloud(stream, points, capacity);
   });
 }
 
@@ -865,6 +885,34 @@ int qm_fuse(float *depth, float *seeds_in, float *seeds_out, const float T_incom
     qm::check(cudaMemsetAsync(workspace, 0xff, fuse_workspace(width, height), as_stream(stream)),
               "workspace reset");
     run_stage(J, q, stage_shape(width, height, q, 1, cam), "fuse", stream);
+  });
+}
+
+int qm_point_cloud_workspace_size(int width, int height, size_t *bytes)
+{
+  return guarded([&] {
+    check_stage_size(width, height);
+    require(bytes != nullptr, "NULL argument");
+    *bytes = qm::point_cloud_workspace(width, height);
+  });
+}
+
+int qm_point_cloud(const float *depth, size_t depth_stride, const uint8_t *ref, size_t ref_pitch,
+                   int width, int height, const qm_camera *cam, const float T_world_ref[12],
+                   float *points, int *count, void *workspace, size_t workspace_bytes,
+                   void *stream)
+{
+  return guarded([&] {
+    check_stage_size(width, height);
+    require(depth && ref && cam && T_world_ref && points && count, "NULL argument");
+    require(depth_stride >= (size_t)width && ref_pitch >= (size_t)width, "bad stride");
+    if (workspace_bytes < qm::point_cloud_workspace(width, height) || !workspace)
+      throw CudaError{QM_ERR_WORKSPACE, "point-cloud workspace too small"};
+    qm::Cam c{cam->fx, cam->fy, cam->cx, cam->cy};
+    qm::launch_point_cloud(depth, depth_stride, ref, ref_pitch, width, height, c, T_world_ref,
+                           reinterpret_cast<float4 *>(points), count, workspace,
+                           as_stream(stream));
+    qm::check(cudaGetLastError(), "point cloud");
   });
 }
 

@@ -78,6 +78,15 @@ void launch_fuse_update(const Batch &B, int blocks, cudaStream_t s);
 // out[i] = seeds[i].w (the fused variance sigma^2), n pixels
 void launch_seed_variance(const float4 *seeds, float *out, long n, cudaStream_t s);
 
+// Point cloud of one depth map (k_points.cu): out receives (x, y, z,
+// intensity) per kept pixel in row-major order, *count (device) their number;
+// ws holds point_cloud_workspace(W, H) bytes.
+int point_cloud_tiles(int W, int H);
+size_t point_cloud_workspace(int W, int H);
+void launch_point_cloud(const float *depth, size_t stride, const uint8_t *ref, size_t pitch, int W,
+                        int H, const Cam &cam, const float *T_world_ref, float4 *out, int *count,
+                        void *ws, cudaStream_t s);
+
 // ---------------------------------------------------------------------------
 // Differentiable path (k_diff.cu).
 

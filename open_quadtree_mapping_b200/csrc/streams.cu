@@ -17,6 +17,7 @@
 // over instead of copying the image.
 #include "streams.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -159,6 +160,8 @@ StreamSet::~StreamSet()
   for (auto &s : st_)
     if (s.pool)
       cudaFree(s.pool);
+  if (pc_buf_)
+    cudaFree(pc_buf_);
 }
 
 bool StreamSet::need_add_reference(const State &s) const
@@ -431,6 +434,41 @@ void StreamSet::get_variance(int i, float *out, size_t stride)
                           s.d.W * sizeof(float), s.d.H, cudaMemcpyDeviceToHost, eng_->stream()),
         "variance download");
   check(cudaStreamSynchronize(eng_->stream()), "variance download");
+}
+
+int StreamSet::get_point_cloud(int i, float *out, size_t capacity)
+{
+  wait();
+  const State &s = st_[i];
+  if (!s.has_ref)
+    throw CudaError{QM_ERR_STATE, "no result yet"};
+  const int W = s.d.W, H = s.d.H;
+  // one device buffer for every stream: points of the largest image, the
+  // count and the scan workspace (allocated on the first call)
+  size_t need = 0;
+  for (const auto &t : st_)
+    need = std::max(need, (size_t)t.d.W * t.d.H * sizeof(float4) + 256 +
+                              point_cloud_workspace(t.d.W, t.d.H));
+  if (!pc_buf_)
+  {
+    check(cudaMalloc(&pc_buf_, need), "point-cloud buffer");
+    pc_bytes_ = need;
+  }
+  float4 *pts = reinterpret_cast<float4 *>(pc_buf_);
+  char *tail = reinterpret_cast<char *>(pc_buf_) + (((size_t)W * H * sizeof(float4) + 255) & ~size_t(255));
+  int *d_count = reinterpret_cast<int *>(tail);
+  void *ws = tail + 256;
+  launch_point_cloud(device_depth(i), (size_t)W, ref_ptr(s), (size_t)W, W, H, s.d.cam,
+                     s.T_world_ref.d, pts, d_count, ws, eng_->stream());
+  check(cudaGetLastError(), "point cloud");
+  int n = 0;
+  check(cudaMemcpyAsync(&n, d_count, sizeof(int), cudaMemcpyDeviceToHost, eng_->stream()),
+        "point count");
+  check(cudaStreamSynchronize(eng_->stream()), "point cloud");
+  const size_t take = std::min((size_t)n, capacity);
+  if (take > 0)
+    check(cudaMemcpy(out, pts, take * sizeof(float4), cudaMemcpyDeviceToHost), "point download");
+  return n;
 }
 
 void StreamSet::get_debug(int i, float *out, size_t stride)

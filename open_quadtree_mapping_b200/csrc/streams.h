@@ -63,6 +63,10 @@ public:
   // fused variance sigma^2 of every pixel of the last result
   void get_variance(int i, float *out, size_t stride);
   void get_reference(int i, uint8_t *out, size_t stride);
+  // point cloud of the last result (Publisher::publishPointCloud,
+  // publisher.cpp:129-166): up to `capacity` points of 4 floats (x, y, z,
+  // intensity) into out; returns the number of points
+  int get_point_cloud(int i, float *out, size_t capacity);
   // fused depth of several streams: all downloads enqueued, one wait
   void get_depths(const int *streams, int n, float *const *outs, const size_t *strides);
   void get_T_world_ref(int i, float *T) const;
@@ -133,6 +137,8 @@ private:
   std::vector<std::pair<int, int>> pending_[2]; // (stream, slot)
   bool inflight_[2] = {false, false};
   long step_ = 0;
+  void *pc_buf_ = nullptr; // point-cloud staging (first get_point_cloud)
+  size_t pc_bytes_ = 0;
 };
 
 } // namespace qm

@@ -91,6 +91,17 @@ class Depthmap:
         _lib.check(_lib.lib().qm_depthmap_get_variance(self._h, out.ctypes.data, self.width))
         return out
 
+    def getPointCloud(self) -> np.ndarray:
+        """(N, 4) float32 rows (x, y, z, intensity) in world coordinates of
+        the last result, as Publisher::publishPointCloud builds them
+        (publisher.cpp:129-166)."""
+        out = np.empty((self.height * self.width, 4), np.float32)
+        n = ctypes.c_int()
+        _lib.check(_lib.lib().qm_depthmap_get_point_cloud(self._h, out.ctypes.data,
+                                                          self.height * self.width,
+                                                          ctypes.byref(n)))
+        return out[:n.value].copy()
+
     def getReferenceImage(self) -> np.ndarray:
         out = np.empty((self.height, self.width), np.uint8)
         _lib.check(_lib.lib().qm_depthmap_get_reference(self._h, out.ctypes.data, self.width))
@@ -244,6 +255,15 @@ class BatchDepthmap:
         out = np.empty((H, W), np.float32)
         _lib.check(_lib.lib().qm_batch_get_variance(self._h, i, out.ctypes.data, W))
         return out
+
+    def get_point_cloud(self, i) -> np.ndarray:
+        """Point cloud of stream i's last result ((N, 4): x, y, z, intensity)."""
+        H, W = self.shapes[i]
+        out = np.empty((H * W, 4), np.float32)
+        n = ctypes.c_int()
+        _lib.check(_lib.lib().qm_batch_get_point_cloud(self._h, i, out.ctypes.data, H * W,
+                                                       ctypes.byref(n)))
+        return out[:n.value].copy()
 
     def get_debug(self, i) -> np.ndarray:
         H, W = self.shapes[i]

@@ -124,6 +124,30 @@ def fuse(depth: torch.Tensor, seeds: torch.Tensor, T_income_last, cam,
     return d, s_in, s_out, table
 
 
+def point_cloud(depth: torch.Tensor, ref: torch.Tensor, cam, T_world_ref) -> torch.Tensor:
+    """Point cloud of a depth map (publisher.cpp:146-163): depth (H, W) f32
+    and ref (H, W) u8 CUDA tensors (row strides may exceed W); returns the
+    (N, 4) f32 CUDA tensor of (x, y, z, intensity) rows in pixel order."""
+    if not (isinstance(depth, torch.Tensor) and depth.is_cuda and depth.dtype == torch.float32
+            and depth.dim() == 2 and depth.stride(1) == 1):
+        raise ValueError("depth must be a row-major CUDA float32 tensor")
+    if not (isinstance(ref, torch.Tensor) and ref.is_cuda and ref.dtype == torch.uint8
+            and ref.dim() == 2 and ref.stride(1) == 1):
+        raise ValueError("ref must be a row-major CUDA uint8 tensor")
+    H, W = depth.shape
+    pts = torch.empty((H * W, 4), dtype=torch.float32, device=depth.device)
+    count = torch.zeros(1, dtype=torch.int32, device=depth.device)
+    nbytes = ctypes.c_size_t()
+    _lib.check(_lib.lib().qm_point_cloud_workspace_size(W, H, ctypes.byref(nbytes)))
+    ws = torch.empty(nbytes.value, dtype=torch.uint8, device=depth.device)
+    T = np.ascontiguousarray(np.asarray(T_world_ref, dtype=np.float32).reshape(12))
+    c = _lib.QmCamera(*[float(v) for v in cam])
+    _lib.check(_lib.lib().qm_point_cloud(_ptr(depth), depth.stride(0), _ptr(ref), ref.stride(0),
+                                         W, H, ctypes.byref(c), T.ctypes.data, _ptr(pts),
+                                         _ptr(count), _ptr(ws), nbytes.value, _stream()))
+    return pts[:int(count.item())]
+
+
 def extract_depth(ref, slots, T_slot_ref, cam, params: Params = Params(),
                   want_messages=False):
     """quadtree -> cost -> BP/extraction -> upsampling on one keyframe."""

@@ -257,3 +257,11 @@ def make_sequence(stream: int, n: int, W=752, H=480, fx=460.0, fy=460.0, cx=None
         gts.append(gt)
         Ts.append(inv_se3(T)[:3, :4].reshape(-1))
     return np.stack(imgs), np.array(Ts, dtype=np.float32), np.stack(gts)
+
+
+def render_frame(args):
+    """(scene seed, T_world_cam, W, H, f) -> u8 image with the principal point
+    at the image centre; a picklable job for process pools."""
+    seed, T, W, H, f = args
+    img, _ = render(make_scene(seed), T, W, H, f, f, W / 2.0, H / 2.0)
+    return img

@@ -165,6 +165,21 @@ def fuse(depth, seeds, T_income_last, cam):
     return out, new_seeds, table, contested
 
 
+def point_cloud(depth, ref, cam, T_world_ref):
+    """Point cloud of a depth map (publisher.cpp:146-163): (N, 4) float32
+    rows (x, y, z, intensity) in row-major pixel order."""
+    depth = np.ascontiguousarray(depth, np.float32)
+    H, W = depth.shape
+    ref = np.ascontiguousarray(ref, np.uint8)
+    T = np.ascontiguousarray(T_world_ref, np.float32).reshape(12)
+    out = np.zeros((H * W, 4), np.float32)
+    fn = lib().orc_point_cloud
+    fn.restype = ctypes.c_int
+    fx, fy, cx, cy = [ctypes.c_float(v) for v in cam]
+    n = fn(_p(depth), _p(ref), W, H, fx, fy, cx, cy, _p(T), _p(out))
+    return out[:n].copy()
+
+
 def slots_from_ring(n_slots: int):
     """Ring index read by measurement slot f: floor(age/10 * f) with the age
     table all zero, i.e. age clamped to 9 (depth_extract.cu:153-166)."""

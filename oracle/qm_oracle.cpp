@@ -912,4 +912,38 @@ void orc_upsample_weights_f32(const uint8_t *img, int W, int H, const orc_params
 ORC_FUSE(orc_fuse_f32, float)
 ORC_FUSE(orc_fuse_f64, double)
 
+// Point cloud of a depth map, Publisher::publishPointCloud
+// (publisher.cpp:146-163): a pixel is kept unless its depth is below 0.1
+// (the float compared as a double); its point is T * (n * depth) with n the
+// unit ray ((x-cx)/fx, (y-cy)/fy, 1) scaled by 1/sqrt of its squared length
+// (helper_math.h normalize with the host rsqrtf, :62-65,1364-1368), the rigid
+// transform applied as a rotation, summed left to right, then the
+// translation (se3.cuh:122-151).  Writes 4 floats (x, y, z, intensity) per
+// point in row-major pixel order; returns the number of points.
+int orc_point_cloud(const float *depth, const uint8_t *ref, int W, int H, float fx, float fy,
+                    float cx, float cy, const float *T, float *xyzi)
+{
+  int n = 0;
+  for (int y = 0; y < H; ++y)
+    for (int x = 0; x < W; ++x)
+    {
+      const float d = depth[(size_t)y * W + x];
+      if ((double)d < 0.1)
+        continue;
+      const float u = ((float)x - cx) / fx;
+      const float v = ((float)y - cy) / fy;
+      const float inv = 1.0f / std::sqrt(u * u + v * v + 1.0f);
+      const float p[3] = {u * inv * d, v * inv * d, inv * d};
+      float *o = xyzi + 4 * (size_t)n;
+      for (int r = 0; r < 3; ++r)
+      {
+        const float rot = T[4 * r] * p[0] + T[4 * r + 1] * p[1] + T[4 * r + 2] * p[2];
+        o[r] = rot + T[4 * r + 3];
+      }
+      o[3] = (float)ref[(size_t)y * W + x];
+      ++n;
+    }
+  return n;
+}
+
 } // extern "C"

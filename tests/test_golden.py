@@ -75,3 +75,18 @@ def test_oracle_fuse_vs_reference_kernels(oracle_mod):
     assert np.array_equal(t2[ok], z["table2"][ok])
     assert np.array_equal(d2[ok], z["fused2"][ok])
     assert np.allclose(s2[ok], z["seeds2"][ok], rtol=2e-5, atol=1e-7)
+
+
+def test_oracle_point_cloud_vs_reference_host_arithmetic(oracle_mod):
+    """tests/golden/ref_pointcloud_160x128.npz holds the publisher's point
+    cloud evaluated with the reference's own helper_math.h / se3.cuh host
+    arithmetic (tests/golden/make_pointcloud_golden.py): the oracle matches
+    it bit for bit, NaN depths (kept by the reference's `< 0.1` test) and the
+    0.1 cut included."""
+    z = _load("ref_pointcloud_160x128")
+    pts = oracle_mod.point_cloud(z["depth"], z["ref"], tuple(float(c) for c in z["cam"]),
+                                 z["T_world_ref"])
+    want = z["points"]
+    assert len(want) > 1000 and np.isnan(want[:, 0]).sum() == 8
+    assert pts.shape == want.shape
+    assert np.array_equal(pts.view(np.uint32), want.view(np.uint32))
