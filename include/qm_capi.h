@@ -117,6 +117,12 @@ int qm_depthmap_get_variance(qm_depthmap *h, float *out, size_t stride);
 int qm_depthmap_get_reference(qm_depthmap *h, uint8_t *out, size_t stride);
 /* getT_world_ref (depthmap.h:74). */
 int qm_depthmap_get_T_world_ref(qm_depthmap *h, float T[12]);
+/* 1 = run the semi-dense tracker on every frame (SeedMatrix::add_frames,
+ * seed_matrix.cu:120-140): its projected depths seed the upsampler's sparse
+ * input and appear in the debug map beside the BP node depths, as in the
+ * reference.  0 (the default) = BP node depths only.  Only before the first
+ * frame (QM_ERR_STATE after). */
+int qm_depthmap_set_semidense(qm_depthmap *h, int enable);
 /* Publisher::publishPointCloud (publisher.cpp:129-166) on the last result:
  * every pixel of the fused depth not below 0.1 gives the point
  * T_world_ref * (normalize(((x-cx)/fx, (y-cy)/fy, 1)) * depth) with the
@@ -183,6 +189,8 @@ int qm_batch_run_resident(qm_batch *b);
 int qm_batch_device_depth(qm_batch *b, int stream, const float **dev_ptr);
 /* 1 = replay captured CUDA graphs (default), 0 = launch stage by stage. */
 int qm_batch_set_graphs(qm_batch *b, int enable);
+/* qm_depthmap_set_semidense for every stream of the batch. */
+int qm_batch_set_semidense(qm_batch *b, int enable);
 /* L2 budget, in bytes, of a job range of the belief propagation: each BP
  * level runs over consecutive streams whose level costs and messages fit in
  * it, so the range's half-sweeps hit L2.  0 = every level over all streams
@@ -310,6 +318,38 @@ int qm_point_cloud(const float *depth, size_t depth_stride, const uint8_t *ref, 
                    int width, int height, const qm_camera *cam, const float T_world_ref[12],
                    float *points, int *count, void *workspace, size_t workspace_bytes,
                    void *stream);
+
+/* ------------------------------------------------ semi-dense tracker ----
+ * The reference's LSD-style keyframe seeds (lsd_semidense.cu, seed_init.cu;
+ * host sequence seed_matrix.cu:106-146,211-446) whose projection into the
+ * incoming frame is the sparse depth the upsampler starts from.  Where the
+ * reference's kernels race (in-place regularisation and hole filling,
+ * propagation by atomicCAS with five retries, last-writer-wins projection)
+ * this library is deterministic: neighbourhood passes read the state before
+ * the pass, a propagation collision keeps the largest inverse depth and a
+ * projection collision the smallest depth. */
+#define QM_SD_INIT 1   /* first frame: seeds from the incoming image */
+#define QM_SD_UPDATE 2 /* update_keyframe: stereo update, hole filling,
+                          regularisation, projection */
+#define QM_SD_SWITCH 3 /* update, then create_new_keyframe: propagation into
+                          the incoming frame, which becomes the keyframe */
+/* One step on device buffers.  key / inc: u8 width x height (dense rows), the
+ * keyframe and the incoming frame (key unused for QM_SD_INIT).
+ * T_income_key: HOST 12 floats, the keyframe-to-incoming transform
+ * (income_transform * keyframe_transform.inv()).  trk / dep: device float4
+ * per pixel, in and out: (valid > 0, blacklist, validity counter, 0) and
+ * (idepth, variance, smooth idepth, smooth variance); zero-filled before the
+ * first step.  debug: device f32 per pixel, out: the projected depths of the
+ * confident seeds in the incoming frame, 0 elsewhere.  arith: QM_ARITH_*
+ * (reference: the texture unit samples the images, as in the reference
+ * kernels; IEEE: software bilinear with 8-bit weights, bit-exact with the
+ * CPU oracle).  In reference arithmetic the call waits for the stream (its
+ * texture objects live for the call). */
+int qm_semidense_workspace_size(int width, int height, size_t *bytes);
+int qm_semidense_step(const uint8_t *key, const uint8_t *inc, int width, int height,
+                      const qm_camera *cam, const float T_income_key[12], int mode, int arith,
+                      float *trk, float *dep, float *debug, void *workspace,
+                      size_t workspace_bytes, void *stream);
 
 /* ------------------------------------------------- differentiable path ----
  * For fitting the BP penalties (P1, P2) and per-pixel upsampling weight

@@ -116,6 +116,9 @@ public:
   {
     qm_check(qm_depthmap_get_reference(h_, out, stride));
   }
+  // Runs the semi-dense tracker on every frame (before the first frame), as
+  // the reference's add_frames does; its depths seed the upsampler.
+  void setSemidense(bool on) { qm_check(qm_depthmap_set_semidense(h_, on ? 1 : 0)); }
   // The cloud Publisher::publishPointCloud builds from the last result
   // (publisher.cpp:129-166): (x, y, z, intensity) per point, world frame.
   std::vector<float> getPointCloud() const

@@ -84,6 +84,8 @@ _SIGS = {
     "qm_batch_run_resident": (_I, [_P]),
     "qm_batch_device_depth": (_I, [_P, _I, ctypes.POINTER(_P)]),
     "qm_batch_set_graphs": (_I, [_P, _I]),
+    "qm_batch_set_semidense": (_I, [_P, _I]),
+    "qm_depthmap_set_semidense": (_I, [_P, _I]),
     "qm_batch_set_group_bytes": (_I, [_P, _S]),
     "qm_batch_set_autotune": (_I, [_P, _I]),
     "qm_batch_set_tune": (_I, [_P, ctypes.POINTER(_I)]),
@@ -101,6 +103,9 @@ _SIGS = {
     "qm_upsample_noalloc": (_I, [_P, _P, _S, _I, _I, ctypes.POINTER(QmParamsC), _P, _P]),
     "qm_fuse_workspace_size": (_I, [_I, _I, ctypes.POINTER(_S)]),
     "qm_point_cloud_workspace_size": (_I, [_I, _I, ctypes.POINTER(_S)]),
+    "qm_semidense_workspace_size": (_I, [_I, _I, ctypes.POINTER(_S)]),
+    "qm_semidense_step": (_I, [_P, _P, _I, _I, ctypes.POINTER(QmCamera), _P, _I, _I, _P, _P, _P,
+                               _P, _S, _P]),
     "qm_point_cloud": (_I, [_P, _S, _P, _S, _I, _I, ctypes.POINTER(QmCamera), _P, _P, _P, _P,
                             _S, _P]),
     "qm_fuse": (_I, [_P, _P, _P, _P, ctypes.POINTER(QmCamera), _I, _I,

@@ -5,6 +5,7 @@
 #include <cstring>
 #include <new>
 
+#include "semidense.h"
 #include "streams.h"
 
 namespace qm
@@ -477,6 +478,15 @@ int qm_depthmap_get_T_world_ref(qm_depthmap *h, float T[12])
   });
 }
 
+int qm_depthmap_set_semidense(qm_depthmap *h, int enable)
+{
+  return guarded([&] {
+    require(h != nullptr, "NULL handle");
+    std::lock_guard<std::mutex> lock(h->set->mutex());
+    h->set->set_semidense(enable != 0);
+  });
+}
+
 int qm_depthmap_get_point_cloud(qm_depthmap *h, float *points, size_t capacity, int *count)
 {
   return guarded([&] {
@@ -621,6 +631,15 @@ int qm_batch_device_depth(qm_batch *b, int stream, const float **dev_ptr)
     std::lock_guard<std::mutex> lock(b->set->mutex());
     b->set->wait();
     *dev_ptr = b->set->device_depth(stream);
+  });
+}
+
+int qm_batch_set_semidense(qm_batch *b, int enable)
+{
+  return guarded([&] {
+    require(b != nullptr, "NULL handle");
+    std::lock_guard<std::mutex> lock(b->set->mutex());
+    b->set->set_semidense(enable != 0);
   });
 }
 
@@ -913,6 +932,112 @@ int qm_point_cloud(const float *depth, size_t depth_stride, const uint8_t *ref, 
                            reinterpret_cast<float4 *>(points), count, workspace,
                            as_stream(stream));
     qm::check(cudaGetLastError(), "point cloud");
+  });
+}
+
+// ------------------------------------------------------ semi-dense tracker
+
+namespace
+{
+
+struct SdLayout
+{
+  size_t pitch, key_f, inc_f, trk2, dep2, zkey, total;
+};
+
+SdLayout sd_layout(int W, int H)
+{
+  auto a512 = [](size_t x) { return (x + 511) & ~size_t(511); };
+  SdLayout L;
+  L.pitch = qm::sd_texture_pitch(W);
+  const size_t img = a512(L.pitch * H * sizeof(float));
+  const size_t P = (size_t)W * H;
+  L.key_f = 0;
+  L.inc_f = L.key_f + img;
+  L.trk2 = L.inc_f + img;
+  L.dep2 = L.trk2 + a512(P * sizeof(float4));
+  L.zkey = L.dep2 + a512(P * sizeof(float4));
+  L.total = L.zkey + a512(P * sizeof(unsigned long long));
+  return L;
+}
+
+} // namespace
+
+int qm_semidense_workspace_size(int width, int height, size_t *bytes)
+{
+  return guarded([&] {
+    check_stage_size(width, height);
+    require(bytes != nullptr, "NULL argument");
+    *bytes = sd_layout(width, height).total;
+  });
+}
+
+int qm_semidense_step(const uint8_t *key, const uint8_t *inc, int width, int height,
+                      const qm_camera *cam, const float T_income_key[12], int mode, int arith,
+                      float *trk, float *dep, float *debug, void *workspace,
+                      size_t workspace_bytes, void *stream)
+{
+  return guarded([&] {
+    check_stage_size(width, height);
+    require(inc && cam && T_income_key && trk && dep && debug, "NULL argument");
+    require(mode == QM_SD_INIT || mode == QM_SD_UPDATE || mode == QM_SD_SWITCH, "bad mode");
+    require(mode == QM_SD_INIT || key != nullptr, "keyframe image missing");
+    require(arith == QM_ARITH_REFERENCE || arith == QM_ARITH_IEEE, "bad arith");
+    const SdLayout L = sd_layout(width, height);
+    if (!workspace || workspace_bytes < L.total)
+      throw CudaError{QM_ERR_WORKSPACE, "semi-dense workspace too small"};
+    const cudaStream_t s = as_stream(stream);
+    char *ws = static_cast<char *>(workspace);
+    qm::SdBatch B;
+    std::memset(&B, 0, sizeof(B));
+    qm::SdJob &J = B.one;
+    J.W = width;
+    J.H = height;
+    J.fx = cam->fx;
+    J.fy = cam->fy;
+    J.cx = cam->cx;
+    J.cy = cam->cy;
+    J.mode = mode;
+    J.inc = inc;
+    J.inc_f = reinterpret_cast<float *>(ws + L.inc_f);
+    J.key_f = reinterpret_cast<float *>(ws + L.key_f);
+    J.pitch = L.pitch;
+    J.trk[0] = reinterpret_cast<float4 *>(trk);
+    J.dep[0] = reinterpret_cast<float4 *>(dep);
+    J.trk[1] = reinterpret_cast<float4 *>(ws + L.trk2);
+    J.dep[1] = reinterpret_cast<float4 *>(ws + L.dep2);
+    J.cur = 0;
+    J.debug = debug;
+    J.zkey = reinterpret_cast<unsigned long long *>(ws + L.zkey);
+    std::memcpy(J.T, T_income_key, 12 * sizeof(float));
+    qm::check(cudaMemsetAsync(J.zkey, 0xff, (size_t)width * height * sizeof(unsigned long long), s),
+              "workspace reset");
+    if (key)
+      qm::launch_u8_to_f32(key, width, height, const_cast<float *>(J.key_f), L.pitch, s);
+    const bool ref = arith == QM_ARITH_REFERENCE;
+    if (ref)
+    {
+      J.key_tex = qm::sd_make_texture(J.key_f, width, height, L.pitch);
+      J.inc_tex = qm::sd_make_texture(J.inc_f, width, height, L.pitch);
+      if (!J.key_tex || !J.inc_tex)
+      {
+        if (J.key_tex)
+          cudaDestroyTextureObject(J.key_tex);
+        if (J.inc_tex)
+          cudaDestroyTextureObject(J.inc_tex);
+        throw CudaError{QM_ERR_CUDA, "texture object creation failed"};
+      }
+    }
+    qm::launch_semidense(B, qm::sd_blocks(width, height), ref ? 0 : 1, s);
+    const cudaError_t e = cudaGetLastError();
+    if (ref)
+    {
+      const cudaError_t w = cudaStreamSynchronize(s);
+      cudaDestroyTextureObject(J.key_tex);
+      cudaDestroyTextureObject(J.inc_tex);
+      qm::check(w, "semi-dense step");
+    }
+    qm::check(e, "semi-dense step");
   });
 }
 

@@ -166,6 +166,13 @@ public:
   void set_group_bytes(size_t bytes) { group_bytes_ = bytes; }
   size_t group_bytes() const { return group_bytes_; }
   int last_launches() const { return last_launches_; }
+  // 1: the sparse buffers arrive filled with the semi-dense tracker's depths
+  // (the quadtree pass keeps them instead of clearing)
+  void set_keep_sparse(bool on)
+  {
+    for (auto &J : master_)
+      J.keep_sparse = on ? 1 : 0;
+  }
   // Launch shapes of the BP and line-solver kernels.  With autotune on (the
   // default) each active job set times three candidates per kernel family
   // on its first run and keeps the fastest; set_tune fixes the shapes for

@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(256)
       o += side * side;
     }
     J.levels[(size_t)y * J.W + x] = (uint8_t)max(level, kp.qt_min);
-    if (J.sparse)
+    if (J.sparse && !J.keep_sparse)
       J.sparse[(size_t)y * J.W + x] = 0.0f; // the debug image starts empty
 
   }
@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(kQtWarps * 32)
       const int level = ok1[c >> 1] ? upper : 0;
       const size_t o = (size_t)(y0 + r) * W + x0 + c;
       J.levels[o] = (uint8_t)max(level, kp.qt_min);
-      if (J.sparse)
+      if (J.sparse && !J.keep_sparse)
         J.sparse[o] = 0.0f; // the debug image starts empty
     }
 }

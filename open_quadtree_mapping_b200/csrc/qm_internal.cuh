@@ -70,6 +70,8 @@ struct JobDesc
   unsigned long long *zkey; // W*H z-buffer keys (all ones = empty)
   int32_t *table;           // W*H fusion source index (0 = none)
   float Tf[12];             // T_income<-lastfuse
+  int keep_sparse;          // 1: `sparse` already holds this frame's
+                            // semi-dense depths (the quadtree pass keeps them)
 };
 
 // The jobs of one launch.  Batched runs keep the job array, the per-stage

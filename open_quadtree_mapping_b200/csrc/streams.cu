@@ -162,6 +162,127 @@ StreamSet::~StreamSet()
       cudaFree(s.pool);
   if (pc_buf_)
     cudaFree(pc_buf_);
+  for (auto &s : st_)
+    for (int k = 0; k < 2; ++k)
+    {
+      if (s.sd_tex[k])
+        cudaDestroyTextureObject(s.sd_tex[k]);
+      if (s.sd_img[k])
+        cudaFree(s.sd_img[k]);
+      if (s.sd_trk[k])
+        cudaFree(s.sd_trk[k]);
+      if (s.sd_dep[k])
+        cudaFree(s.sd_dep[k]);
+    }
+  for (int q = 0; q < 2; ++q)
+  {
+    if (h_sdjobs_[q])
+      cudaFreeHost(h_sdjobs_[q]);
+    if (h_sdprefix_[q])
+      cudaFreeHost(h_sdprefix_[q]);
+  }
+  if (d_sdjobs_)
+    cudaFree(d_sdjobs_);
+  if (d_sdprefix_)
+    cudaFree(d_sdprefix_);
+}
+
+void StreamSet::set_semidense(bool on)
+{
+  if (on == semidense_)
+    return;
+  if (started_)
+    throw CudaError{QM_ERR_STATE, "the semi-dense tracker is switched before the first frame"};
+  check(cudaSetDevice(device_), "cudaSetDevice");
+  if (on && !d_sdjobs_)
+  {
+    const int n = size();
+    for (auto &s : st_)
+    {
+      const size_t P = (size_t)s.d.W * s.d.H;
+      s.sd_pitch = sd_texture_pitch(s.d.W);
+      for (int k = 0; k < 2; ++k)
+      {
+        check(cudaMalloc((void **)&s.sd_img[k], s.sd_pitch * s.d.H * sizeof(float)),
+              "semi-dense image allocation");
+        check(cudaMalloc((void **)&s.sd_trk[k], P * sizeof(float4)), "seed allocation");
+        check(cudaMalloc((void **)&s.sd_dep[k], P * sizeof(float4)), "seed allocation");
+        check(cudaMemset(s.sd_img[k], 0, s.sd_pitch * s.d.H * sizeof(float)), "memset");
+        check(cudaMemset(s.sd_trk[k], 0, P * sizeof(float4)), "memset");
+        check(cudaMemset(s.sd_dep[k], 0, P * sizeof(float4)), "memset");
+        s.sd_tex[k] = sd_make_texture(s.sd_img[k], s.d.W, s.d.H, s.sd_pitch);
+        if (!s.sd_tex[k])
+          throw CudaError{QM_ERR_CUDA, "texture object creation failed"};
+      }
+    }
+    for (int q = 0; q < 2; ++q)
+    {
+      check(cudaHostAlloc((void **)&h_sdjobs_[q], sizeof(SdJob) * n, cudaHostAllocDefault),
+            "pinned allocation");
+      check(cudaHostAlloc((void **)&h_sdprefix_[q], sizeof(int) * (n + 1), cudaHostAllocDefault),
+            "pinned allocation");
+    }
+    check(cudaMalloc((void **)&d_sdjobs_, sizeof(SdJob) * n), "device allocation");
+    check(cudaMalloc((void **)&d_sdprefix_, sizeof(int) * (n + 1)), "device allocation");
+  }
+  semidense_ = on;
+  eng_->set_keep_sparse(on);
+}
+
+void StreamSet::semidense_step(const std::vector<int> &which, int parity)
+{
+  SdJob *jobs = h_sdjobs_[parity];
+  int *prefix = h_sdprefix_[parity];
+  const bool ieee = eng_->params().arith == QM_ARITH_IEEE;
+  int n = 0;
+  prefix[0] = 0;
+  for (int i : which)
+  {
+    State &s = st_[i];
+    SdJob &J = jobs[n];
+    std::memset(&J, 0, sizeof(J));
+    J.W = s.d.W;
+    J.H = s.d.H;
+    J.fx = s.d.cam.fx;
+    J.fy = s.d.cam.fy;
+    J.cx = s.d.cam.cx;
+    J.cy = s.d.cam.cy;
+    J.mode = s.sd_mode;
+    J.inc = frame_ptr(s, s.income_slot);
+    J.inc_f = s.sd_img[s.sd_key ^ 1];
+    J.key_f = s.sd_img[s.sd_key];
+    J.pitch = s.sd_pitch;
+    J.inc_tex = ieee ? 0 : s.sd_tex[s.sd_key ^ 1];
+    J.key_tex = ieee ? 0 : s.sd_tex[s.sd_key];
+    for (int k = 0; k < 2; ++k)
+    {
+      J.trk[k] = s.sd_trk[k];
+      J.dep[k] = s.sd_dep[k];
+    }
+    J.cur = 0;
+    J.debug = eng_->buffers(i).sparse;
+    J.zkey = eng_->buffers(i).zkey;
+    std::memcpy(J.T, s.sd_T.d, sizeof(J.T));
+    prefix[n + 1] = prefix[n] + sd_blocks(s.d.W, s.d.H);
+    ++n;
+    // the incoming image becomes the keyframe after a first frame or a switch
+    if (s.sd_mode == kSdInit || s.sd_mode == kSdSwitch)
+      s.sd_key ^= 1;
+  }
+  if (n == 0)
+    return;
+  const cudaStream_t cs = eng_->stream();
+  check(cudaMemcpyAsync(d_sdjobs_, jobs, sizeof(SdJob) * n, cudaMemcpyHostToDevice, cs),
+        "semi-dense job upload");
+  check(cudaMemcpyAsync(d_sdprefix_, prefix, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, cs),
+        "semi-dense job upload");
+  SdBatch B;
+  std::memset(&B, 0, sizeof(B));
+  B.jobs = d_sdjobs_;
+  B.prefix = d_sdprefix_;
+  B.njobs = n;
+  launch_semidense(B, prefix[n], ieee ? 1 : 0, cs);
+  check(cudaGetLastError(), "semi-dense launch");
 }
 
 bool StreamSet::need_add_reference(const State &s) const
@@ -201,12 +322,20 @@ StreamSet::Outcome StreamSet::begin_frame(int i, const uint8_t *img, size_t stri
   {
     s.keyframe_T = s.income_T;
     s.initialized = true;
+    s.sd_mode = kSdInit;
+    s.sd_T = SE3f::identity();
     return kFirst;
   }
-  // The keyframe switch only matters to the semi-dense tracker; the pose is
-  // kept so that the stream state mirrors the reference's.
+  // the semi-dense step updates the seeds against the current keyframe
+  // (key_to_income, seed_matrix.cu:417) and then, when the camera moved far
+  // enough, makes this frame the keyframe (seed_matrix.cu:131-140)
+  s.sd_T = s.income_T * s.keyframe_T.inv();
+  s.sd_mode = kSdUpdate;
   if (need_switch_keyframe(s))
+  {
     s.keyframe_T = s.income_T;
+    s.sd_mode = kSdSwitch;
+  }
   if (s.frame_index % s.d.ratio != 0)
     return kSkip;
   if ((int)s.ring.size() <= 10)
@@ -311,6 +440,7 @@ void StreamSet::step(const std::vector<int> &which, const uint8_t *const *imgs,
   if (inflight_[p ^ 1])
     check(cudaEventSynchronize(ev_up_[p ^ 1]), "upload");
   eng_->set_parity(p);
+  started_ = true;
   std::vector<int> active;
   for (size_t k = 0; k < which.size(); ++k)
   {
@@ -321,6 +451,8 @@ void StreamSet::step(const std::vector<int> &which, const uint8_t *const *imgs,
   }
   check(cudaEventRecord(ev_up_[p], up_), "event");
   check(cudaStreamWaitEvent(eng_->stream(), ev_up_[p], 0), "event wait");
+  if (semidense_)
+    semidense_step(which, p);
   if (!active.empty())
   {
     eng_->launch(active);

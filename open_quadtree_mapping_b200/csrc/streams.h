@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "semidense.h"
 
 namespace qm
 {
@@ -55,6 +56,11 @@ public:
   void wait();
   // Single-stream form used by the Depthmap facade.
   int add_frame(int i, const uint8_t *img, size_t stride, const float *T_curr_world);
+  // Runs the semi-dense tracker on every frame of every stream, its
+  // projected depths seeding the upsampler (as the reference's add_frames
+  // does).  Only before the first frame.
+  void set_semidense(bool on);
+  bool semidense() const { return semidense_; }
   void run_resident();
   void profile_resident(float *ms, int *launches);
 
@@ -105,6 +111,16 @@ private:
     bool has_ref = false; // the pool's last slot holds the last result's image
     int out_parity = 0;   // output buffer of the last result
     SE3f T_world_ref;
+    // semi-dense tracker: float images (keyframe / incoming, roles swap on a
+    // keyframe switch) with their texture views, seeds (two buffers each of
+    // trk and dep), and this frame's step
+    float *sd_img[2] = {nullptr, nullptr};
+    cudaTextureObject_t sd_tex[2] = {0, 0};
+    size_t sd_pitch = 0;
+    float4 *sd_trk[2] = {nullptr, nullptr}, *sd_dep[2] = {nullptr, nullptr};
+    int sd_key = 0; // sd_img index of the keyframe
+    int sd_mode = kSdNone;
+    SE3f sd_T;      // T_income<-key of this frame's step
   };
 
   Outcome begin_frame(int i, const uint8_t *img, size_t stride, const float *T);
@@ -123,6 +139,9 @@ private:
   }
   uint8_t *ref_ptr(const State &s) const { return frame_ptr(s, QM_RING_CAPACITY + 2); }
   void keep_reference(State &s);
+  // enqueues the semi-dense step of the streams in `which` on the engine
+  // stream (after their uploads)
+  void semidense_step(const std::vector<int> &which, int parity);
 
   int device_;
   std::vector<State> st_;
@@ -139,6 +158,13 @@ private:
   long step_ = 0;
   void *pc_buf_ = nullptr; // point-cloud staging (first get_point_cloud)
   size_t pc_bytes_ = 0;
+  bool semidense_ = false;
+  bool started_ = false; // a frame has been added
+  // semi-dense job tables: pinned per parity, one device copy
+  SdJob *h_sdjobs_[2] = {nullptr, nullptr};
+  int *h_sdprefix_[2] = {nullptr, nullptr};
+  SdJob *d_sdjobs_ = nullptr;
+  int *d_sdprefix_ = nullptr;
 };
 
 } // namespace qm

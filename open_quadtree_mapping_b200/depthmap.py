@@ -91,6 +91,10 @@ class Depthmap:
         _lib.check(_lib.lib().qm_depthmap_get_variance(self._h, out.ctypes.data, self.width))
         return out
 
+    def set_semidense(self, on: bool) -> None:
+        """Run the semi-dense tracker on every frame (before the first frame)."""
+        _lib.check(_lib.lib().qm_depthmap_set_semidense(self._h, 1 if on else 0))
+
     def getPointCloud(self) -> np.ndarray:
         """(N, 4) float32 rows (x, y, z, intensity) in world coordinates of
         the last result, as Publisher::publishPointCloud builds them
@@ -273,6 +277,11 @@ class BatchDepthmap:
 
     def run_resident(self) -> None:
         _lib.check(_lib.lib().qm_batch_run_resident(self._h))
+
+    def set_semidense(self, on: bool) -> None:
+        """Run the semi-dense tracker on every frame of every stream (before
+        the first frame)."""
+        _lib.check(_lib.lib().qm_batch_set_semidense(self._h, 1 if on else 0))
 
     def set_graphs(self, on: bool) -> None:
         _lib.check(_lib.lib().qm_batch_set_graphs(self._h, 1 if on else 0))

@@ -148,6 +148,33 @@ def point_cloud(depth: torch.Tensor, ref: torch.Tensor, cam, T_world_ref) -> tor
     return pts[:int(count.item())]
 
 
+SD_INIT, SD_UPDATE, SD_SWITCH = 1, 2, 3
+
+
+def semidense_step(key, inc, cam, T_income_key, mode, trk, dep, arith=0):
+    """One semi-dense tracker step (qm_semidense_step).  key / inc: (H, W)
+    uint8 CUDA tensors (key may be None for SD_INIT); trk / dep: (H, W, 4)
+    float32 CUDA tensors updated in place.  Returns the (H, W) float32 debug
+    image (projected depths of the confident seeds, 0 elsewhere)."""
+    _need(inc, torch.uint8, "inc")
+    _need(trk, torch.float32, "trk")
+    _need(dep, torch.float32, "dep")
+    if key is not None:
+        _need(key, torch.uint8, "key")
+    H, W = inc.shape
+    debug = torch.empty((H, W), dtype=torch.float32, device=inc.device)
+    nbytes = ctypes.c_size_t()
+    _lib.check(_lib.lib().qm_semidense_workspace_size(W, H, ctypes.byref(nbytes)))
+    ws = torch.empty(nbytes.value, dtype=torch.uint8, device=inc.device)
+    T = np.ascontiguousarray(np.asarray(T_income_key, dtype=np.float32).reshape(12))
+    c = _lib.QmCamera(*[float(v) for v in cam])
+    _lib.check(_lib.lib().qm_semidense_step(
+        _ptr(key) if key is not None else None, _ptr(inc), W, H, ctypes.byref(c), T.ctypes.data,
+        int(mode), int(arith), _ptr(trk), _ptr(dep), _ptr(debug), _ptr(ws), nbytes.value,
+        _stream()))
+    return debug
+
+
 def extract_depth(ref, slots, T_slot_ref, cam, params: Params = Params(),
                   want_messages=False):
     """quadtree -> cost -> BP/extraction -> upsampling on one keyframe."""

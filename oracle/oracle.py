@@ -180,6 +180,37 @@ def point_cloud(depth, ref, cam, T_world_ref):
     return out[:n].copy()
 
 
+SD_INIT, SD_UPDATE, SD_SWITCH = 1, 2, 3
+
+
+def sd_step(key, inc, cam, T_income_key, mode, trk, dep):
+    """One semi-dense step (qm_oracle_semidense.cpp).  key / inc: (H, W)
+    uint8 (key None for SD_INIT); trk / dep: (H, W, 4) float32, updated in
+    place.  Returns the debug image (H, W) float32."""
+    inc = np.ascontiguousarray(inc, np.uint8)
+    H, W = inc.shape
+    key = None if key is None else np.ascontiguousarray(key, np.uint8)
+    T = np.ascontiguousarray(T_income_key, np.float32).reshape(12)
+    assert trk.dtype == np.float32 and trk.flags.c_contiguous and trk.shape == (H, W, 4)
+    assert dep.dtype == np.float32 and dep.flags.c_contiguous and dep.shape == (H, W, 4)
+    debug = np.zeros((H, W), np.float32)
+    fx, fy, cx, cy = [ctypes.c_float(v) for v in cam]
+    lib().orc_sd_step(W, H, fx, fy, cx, cy, _p(key) if key is not None else None, _p(inc),
+                      _p(T), int(mode), _p(trk), _p(dep), _p(debug))
+    return debug
+
+
+def sd_sample(img, uv):
+    """The oracle's bilinear texture emulation (8-bit fractional weights,
+    clamp) of a u8 image at (n, 2) unnormalised coordinates."""
+    img = np.ascontiguousarray(img, np.uint8)
+    H, W = img.shape
+    uv = np.ascontiguousarray(uv, np.float32).reshape(-1, 2)
+    out = np.zeros(len(uv), np.float32)
+    lib().orc_sd_sample(_p(img), W, H, _p(uv), len(uv), _p(out))
+    return out
+
+
 def slots_from_ring(n_slots: int):
     """Ring index read by measurement slot f: floor(age/10 * f) with the age
     table all zero, i.e. age clamped to 9 (depth_extract.cu:153-166)."""

@@ -64,19 +64,28 @@ class PolicyReplay:
         self.initialized = False
         self.fuse_T = se3_identity()
         self.keyframe_T = se3_identity()
+        self.keyframe_id = None
 
     def add(self, frame_id, T_curr_world):
+        """Every outcome also carries the semi-dense step of the frame:
+        sd_mode (1 first frame, 2 update, 3 update + keyframe switch),
+        sd_key (frame id of the keyframe before the step) and sd_T
+        (T_income<-key)."""
         T = np.asarray(T_curr_world, f32).reshape(12)
         self.frame_index += 1
         if not self.initialized:
             self.initialized = True
             self.keyframe_T = T
-            return dict(outcome="first")
+            self.keyframe_id = frame_id
+            return dict(outcome="first", sd_mode=1, sd_key=None, sd_T=se3_identity())
+        sd = dict(sd_mode=2, sd_key=self.keyframe_id, sd_T=se3_mul(T, se3_inv(self.keyframe_T)))
         if _moved(self.keyframe_T, T, 0.86, 0.5):
             self.keyframe_T = T
+            self.keyframe_id = frame_id
+            sd["sd_mode"] = 3
         if self.frame_index % self.ratio != 0:
-            return dict(outcome="skip")
-        out = dict(outcome="none")
+            return dict(outcome="skip", **sd)
+        out = dict(outcome="none", **sd)
         if len(self.ring) > 10:
             inv = se3_inv(T)
             slots, Ts = [], []
@@ -87,7 +96,7 @@ class PolicyReplay:
                 slots.append(fid)
                 Ts.append(se3_mul(Tf, inv))
             out = dict(outcome="dense", slots=slots, T_slots=np.stack(Ts),
-                       T_fuse=se3_mul(T, se3_inv(self.fuse_T)))
+                       T_fuse=se3_mul(T, se3_inv(self.fuse_T)), **sd)
         if not self.ring or _moved(self.ring[0][1], T, 0.95, 0.03):
             self.ring.insert(0, (frame_id, T))
             if len(self.ring) > self.capacity:

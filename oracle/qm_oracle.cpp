@@ -848,6 +848,7 @@ extern "C" {
 
 // Host threads used by the parallel loops (1 = scalar port).
 void orc_set_threads(int n) { g_threads = n < 1 ? 1 : n; }
+int orc_get_threads(void) { return g_threads; }
 
 void orc_quadtree(const uint8_t *img, int w, int h, const orc_params *p, int *levels)
 {

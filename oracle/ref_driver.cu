@@ -3,7 +3,8 @@
 // This translation unit compiles the reference's own depth-path kernels,
 // unmodified, from the reference source tree (src/quadtree.cu,
 // src/depth_extract.cu, src/bpextract.cu, src/depth_upsample.cu,
-// src/depth_fusion.cu are #included by path; see oracle/Makefile), with the
+// src/depth_fusion.cu, and for the semi-dense tracker src/seed_init.cu and
+// src/lsd_semidense.cu, are #included by path; see oracle/Makefile), with the
 // reference's flags (-O3 -use_fast_math) for sm_100a.  Only the legacy texture
 // references are swapped for texture objects (ref_shim/quadmap/
 // texture_memory.cuh) and <opencv2/opencv.hpp> for an empty header.
@@ -27,7 +28,10 @@
 #include <quadmap/match_parameter.cuh>
 #include <quadmap/texture_memory.cuh>
 #include <quadmap/stereo_parameter.cuh>
+#include <quadmap/DepthSeed.cuh>
 
+#include "seed_init.cu"
+#include "lsd_semidense.cu"
 #include "quadtree.cu"
 #include "depth_extract.cu"
 #include "bpextract.cu"
@@ -356,6 +360,175 @@ int qmref_time_frames(int w, int h, float fx, float fy, float cx, float cy,
         total += std::chrono::duration<double, std::milli>(t1 - t0).count();
     }
     *ms_per_frame = total / iters;
+  }
+  catch (const std::exception &)
+  {
+    return 2;
+  }
+  return status();
+}
+
+__global__ void tex_sample_kernel(cudaTextureObject_t t, const float *uv, int n, float *out)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n)
+    out[k] = tex2D<float>(t, uv[2 * k], uv[2 * k + 1]);
+}
+
+// Samples of a float image (w*h) through a texture object set up as the
+// reference's bindTexture does (linear filtering, clamp, unnormalised
+// coordinates) at n coordinates (x, y pairs).
+int qmref_tex_sample(int w, int h, const float *img, const float *uv, int n, float *out)
+{
+  try
+  {
+    DeviceImage<float> image(w, h);
+    image.setDevData(img);
+    bindTexture(income_image_tex, image);
+    const cudaTextureObject_t t = shim_live_textures()[(const void *)&income_image_tex];
+    float *d_uv = nullptr, *d_out = nullptr;
+    cudaMalloc(&d_uv, sizeof(float) * 2 * n);
+    cudaMalloc(&d_out, sizeof(float) * n);
+    cudaMemcpy(d_uv, uv, sizeof(float) * 2 * n, cudaMemcpyHostToDevice);
+    tex_sample_kernel<<<(n + 255) / 256, 256>>>(t, d_uv, n, d_out);
+    cudaMemcpy(out, d_out, sizeof(float) * n, cudaMemcpyDeviceToHost);
+    cudaFree(d_uv);
+    cudaFree(d_out);
+    cudaUnbindTexture(income_image_tex);
+  }
+  catch (const std::exception &)
+  {
+    return 2;
+  }
+  return status();
+}
+
+// The semi-dense tracker as SeedMatrix::add_frames runs it, frame after
+// frame: initial_keyframe (seed_matrix.cu:211-242) on the first frame, then
+// update_keyframe (:401-446) and, when need_switchkeyframe (:198-209) says
+// so, create_new_keyframe (:246-304) followed by set_income_as_keyframe.
+//   frames       n*w*h float (values 0..255)
+//   T_cur_world  n*12 floats (world -> camera)
+//   debug_out    n*w*h: the debug image after each frame's update
+//   seeds_out    w*h*8 floats or NULL: the seeds after the last frame,
+//                (track_info x, y, z, 0, depth_info x, y, z, w) per pixel
+//   modes_out    n ints: 1 first frame, 2 update, 3 update + keyframe switch
+int qmref_semidense(int w, int h, float fx, float fy, float cx, float cy, int n,
+                    const float *frames, const float *T_cur_world, float *debug_out,
+                    float *seeds_out, int *modes_out)
+{
+  try
+  {
+    const float4 camera_para = make_float4(fx, cx, fy, cy);
+    DeviceImage<float> income_image(w, h), keyframe_image(w, h), debug_image(w, h);
+    DeviceImage<float2> income_gradient(w, h), keyframe_gradient(w, h);
+    DeviceImage<DepthSeed> keyframe_semidense(w, h);
+    keyframe_semidense.zero();
+    income_gradient.zero();
+    keyframe_gradient.zero();
+    SE3<float> income_transform, keyframe_transform;
+    dim3 block(8, 8), grid((w + 7) / 8, (h + 7) / 8);
+    auto bind_all = [&]() {
+      bindTexture(income_image_tex, income_image);
+      bindTexture(income_gradient_tex, income_gradient);
+      bindTexture(keyframe_image_tex, keyframe_image);
+      bindTexture(keyframe_gradient_tex, keyframe_gradient);
+    };
+    auto unbind_all = [&]() {
+      cudaUnbindTexture(income_image_tex);
+      cudaUnbindTexture(income_gradient_tex);
+      cudaUnbindTexture(keyframe_image_tex);
+      cudaUnbindTexture(keyframe_gradient_tex);
+    };
+    for (int i = 0; i < n; ++i)
+    {
+      debug_image.zero();
+      income_image.setDevData(frames + (size_t)i * w * h);
+      income_transform = se3_from(T_cur_world + 12 * i);
+      generate_gradient(income_image, income_gradient);
+      cudaDeviceSynchronize();
+      if (i == 0)
+      {
+        keyframe_image = income_image;
+        keyframe_gradient = income_gradient;
+        keyframe_transform = income_transform;
+        bind_all();
+        initialize_keyframe_kernel<<<grid, block>>>(keyframe_semidense.dev_ptr);
+        cudaDeviceSynchronize();
+        unbind_all();
+        modes_out[i] = 1;
+        debug_image.getDevData(debug_out + (size_t)i * w * h);
+        continue;
+      }
+      bind_all();
+      const SE3<float> key_to_income = income_transform * keyframe_transform.inv();
+      update_keyframe_kernel<<<grid, block>>>(keyframe_semidense.dev_ptr, camera_para,
+                                              key_to_income, debug_image.dev_ptr);
+      regulizeDepth_FillHoles_kernel<<<grid, block>>>(keyframe_semidense.dev_ptr);
+      regulizeDepth_kernel<<<grid, block>>>(keyframe_semidense.dev_ptr, false);
+      depth_project_kernel<<<grid, block>>>(keyframe_semidense.dev_ptr, camera_para,
+                                            key_to_income, debug_image.dev_ptr);
+      cudaDeviceSynchronize();
+      unbind_all();
+      debug_image.getDevData(debug_out + (size_t)i * w * h);
+      modes_out[i] = 2;
+      // need_switchkeyframe
+      const SE3<float> keyframe_pose = keyframe_transform.inv();
+      const SE3<float> income_pose = income_transform.inv();
+      const float3 kz = make_float3(keyframe_pose.data(0, 2), keyframe_pose.data(1, 2),
+                                    keyframe_pose.data(2, 2));
+      const float3 iz = make_float3(income_pose.data(0, 2), income_pose.data(1, 2),
+                                    income_pose.data(2, 2));
+      const float z_cos = dot(kz, iz);
+      const float base_line =
+          length(keyframe_pose.getTranslation() - income_pose.getTranslation());
+      if (z_cos < 0.86 || base_line > 0.5)
+      {
+        bind_all();
+        const SE3<float> old_to_new = income_transform * keyframe_transform.inv();
+        DeviceImage<int> transform_table(w, h);
+        DeviceImage<DepthSeed> new_keyframe(w, h);
+        DeviceImage<float3> new_info(w, h);
+        new_keyframe.zero();
+        transform_table.zero();
+        propogate_keyframe_kernel<<<grid, block>>>(keyframe_semidense.dev_ptr, camera_para,
+                                                   old_to_new, transform_table.dev_ptr,
+                                                   new_info.dev_ptr);
+        cudaDeviceSynchronize();
+        initialize_keyframe_kernel<<<grid, block>>>(new_keyframe.dev_ptr,
+                                                    transform_table.dev_ptr, new_info.dev_ptr);
+        cudaDeviceSynchronize();
+        regulizeDepth_kernel<<<grid, block>>>(new_keyframe.dev_ptr, true);
+        cudaDeviceSynchronize();
+        regulizeDepth_FillHoles_kernel<<<grid, block>>>(new_keyframe.dev_ptr);
+        cudaDeviceSynchronize();
+        regulizeDepth_kernel<<<grid, block>>>(new_keyframe.dev_ptr, false);
+        cudaDeviceSynchronize();
+        keyframe_semidense = new_keyframe;
+        unbind_all();
+        keyframe_image = income_image;
+        keyframe_gradient = income_gradient;
+        keyframe_transform = income_transform;
+        modes_out[i] = 3;
+      }
+    }
+    if (seeds_out)
+    {
+      std::vector<DepthSeed> host((size_t)w * h);
+      keyframe_semidense.getDevData(host.data());
+      for (size_t o = 0; o < host.size(); ++o)
+      {
+        float *d = seeds_out + 8 * o;
+        d[0] = host[o].track_info.x;
+        d[1] = host[o].track_info.y;
+        d[2] = host[o].track_info.z;
+        d[3] = 0.0f;
+        d[4] = host[o].depth_info.x;
+        d[5] = host[o].depth_info.y;
+        d[6] = host[o].depth_info.z;
+        d[7] = host[o].depth_info.w;
+      }
+    }
   }
   catch (const std::exception &)
   {

@@ -34,6 +34,11 @@ def lib():
                                     ctypes.c_int, p, p, p, p, p]
         L.qmref_fuse.restype = ctypes.c_int
         L.qmref_fuse.argtypes = [ctypes.c_int, ctypes.c_int, f, f, f, f, p, p, p, p]
+        L.qmref_tex_sample.restype = ctypes.c_int
+        L.qmref_tex_sample.argtypes = [ctypes.c_int, ctypes.c_int, p, p, ctypes.c_int, p]
+        L.qmref_semidense.restype = ctypes.c_int
+        L.qmref_semidense.argtypes = [ctypes.c_int, ctypes.c_int, f, f, f, f, ctypes.c_int, p, p,
+                                      p, p, p]
         L.qmref_time_frames.restype = ctypes.c_int
         L.qmref_time_frames.argtypes = [ctypes.c_int, ctypes.c_int, f, f, f, f, p, ctypes.c_int,
                                         p, p, ctypes.c_int, p, ctypes.c_int, ctypes.c_int,
@@ -132,3 +137,34 @@ def labels_from_messages(cost, msgs, levels, W, H):
     size = 1 << levels[np.ix_(ys, xs)]
     node = ((np.arange(cw)[None, :] * 4) % size == 0) & ((np.arange(ch)[:, None] * 4) % size == 0)
     return np.where(node, lab, -1).astype(np.int32)
+
+
+def semidense(frames, T_cur_world, cam):
+    """The reference's semi-dense tracker over a frame sequence (qmref_semidense):
+    frames (n, H, W) u8, T_cur_world (n, 12).  Returns (debug (n, H, W) f32,
+    seeds (H, W, 8) f32 after the last frame, modes (n,) int32)."""
+    frames = np.ascontiguousarray(frames, np.float32)
+    n, H, W = frames.shape
+    T = np.ascontiguousarray(T_cur_world, np.float32).reshape(n, 12)
+    debug = np.zeros((n, H, W), np.float32)
+    seeds = np.zeros((H, W, 8), np.float32)
+    modes = np.zeros(n, np.int32)
+    fx, fy, cx, cy = [float(v) for v in cam]
+    rc = lib().qmref_semidense(W, H, fx, fy, cx, cy, n, _p(frames), _p(T), _p(debug), _p(seeds),
+                               _p(modes))
+    if rc != 0:
+        raise RuntimeError("qmref_semidense failed: %d" % rc)
+    return debug, seeds, modes
+
+
+def tex_sample(img, uv):
+    """Texture-unit bilinear samples of a u8 image (as float texels) at the
+    (n, 2) unnormalised coordinates uv (qmref_tex_sample)."""
+    img = np.ascontiguousarray(img, np.float32)
+    H, W = img.shape
+    uv = np.ascontiguousarray(uv, np.float32).reshape(-1, 2)
+    out = np.zeros(len(uv), np.float32)
+    rc = lib().qmref_tex_sample(W, H, _p(img), _p(uv), len(uv), _p(out))
+    if rc != 0:
+        raise RuntimeError("qmref_tex_sample failed: %d" % rc)
+    return out

@@ -1,0 +1,178 @@
+"""Semi-dense tracker kernels (qm_semidense_step, through the C-ABI) against
+the oracle (oracle/qm_oracle_semidense.cpp): in IEEE arithmetic every seed
+field and every projected depth is bit-identical frame after frame, keyframe
+switches included; in reference arithmetic (texture-unit sampling and the
+reference build's rounding) the projected depths agree closely."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import sequence
+from open_quadtree_mapping_b200.params import ARITH_IEEE, ARITH_REFERENCE
+from oracle.policy import PolicyReplay
+
+pytestmark = pytest.mark.gpu
+
+
+def _same(a, b):
+    a = np.ascontiguousarray(a, np.float32)
+    b = np.ascontiguousarray(b, np.float32)
+    na, nb = np.isnan(a), np.isnan(b)
+    return bool(np.array_equal(na, nb) and
+                np.array_equal(a[~na].view(np.uint32), b[~nb].view(np.uint32)))
+
+
+def _replay(W, H, n, stream, arith, oracle_mod, dev, check_oracle=True):
+    from open_quadtree_mapping_b200 import stages
+    f = 460.0 * W / 752.0
+    imgs, Ts, gts = sequence(stream, n, W, H)
+    cam = (f, f, W / 2.0, H / 2.0)
+    pol = PolicyReplay()
+    trk_o = np.zeros((H, W, 4), np.float32)
+    dep_o = np.zeros((H, W, 4), np.float32)
+    trk_g = torch.zeros((H, W, 4), dtype=torch.float32, device=dev)
+    dep_g = torch.zeros((H, W, 4), dtype=torch.float32, device=dev)
+    frames = [torch.from_numpy(np.ascontiguousarray(im)).to(dev) for im in imgs]
+    out = []
+    for i in range(n):
+        r = pol.add(i, Ts[i])
+        k = r["sd_key"]
+        dbg_g = stages.semidense_step(frames[k] if k is not None else None, frames[i], cam,
+                                      r["sd_T"], r["sd_mode"], trk_g, dep_g, arith)
+        torch.cuda.synchronize()
+        dbg_o = None
+        if check_oracle:
+            dbg_o = oracle_mod.sd_step(imgs[k] if k is not None else None, imgs[i], cam,
+                                       r["sd_T"], r["sd_mode"], trk_o, dep_o)
+        out.append((r["sd_mode"], dbg_g.cpu().numpy(), trk_g.cpu().numpy(), dep_g.cpu().numpy(),
+                    dbg_o, trk_o.copy(), dep_o.copy(), gts[i]))
+    return out
+
+
+@pytest.mark.parametrize("W,H,n,stream", [(160, 128, 30, 3), (752, 480, 14, 4)])
+def test_semidense_ieee_bit_exact_with_oracle(oracle_mod, gpu, W, H, n, stream):
+    steps = _replay(W, H, n, stream, ARITH_IEEE, oracle_mod, gpu)
+    assert {s[0] for s in steps} >= {1, 2}
+    for i, (mode, dg, tg, pg, do, to, po, gt) in enumerate(steps):
+        assert _same(tg, to), ("seeds (trk)", i, mode)
+        assert _same(pg, po), ("seeds (dep)", i, mode)
+        assert _same(dg, do), ("debug", i, mode)
+    if W == 160:
+        assert 3 in {s[0] for s in steps}  # keyframe switches were exercised
+    # the tracker tracks: projected depths near the ray-cast ground truth
+    dg, gt = steps[-1][1], steps[-1][7]
+    m = dg > 0
+    assert m.sum() > 0.05 * W * H
+    assert np.median(np.abs(dg[m] - gt[m]) / gt[m]) < 0.1
+
+
+def test_semidense_reference_arith_close_to_ieee(oracle_mod, gpu):
+    W, H, n = 160, 128, 20
+    ref = _replay(W, H, n, 3, ARITH_REFERENCE, oracle_mod, gpu, check_oracle=False)
+    iee = _replay(W, H, n, 3, ARITH_IEEE, oracle_mod, gpu, check_oracle=False)
+    for (_, dr, tr, _, _, _, _, gt), (_, di, ti, _, _, _, _, _) in zip(ref, iee):
+        vr, vi = tr[..., 0] > 0, ti[..., 0] > 0
+        assert (vr == vi).mean() > 0.9
+    dr, di, gt = ref[-1][1], iee[-1][1], ref[-1][7]
+    both = (dr > 0) & (di > 0)
+    assert both.sum() > 0.5 * max((dr > 0).sum(), 1)
+    assert np.median(np.abs(dr[both] - di[both]) / di[both]) < 1e-3
+    m = dr > 0
+    assert np.median(np.abs(dr[m] - gt[m]) / gt[m]) < 0.1
+
+
+def test_facade_with_semidense_matches_oracle_replay(oracle_mod, gpu):
+    """Depthmap with the semi-dense tracker on (IEEE arithmetic): on every
+    dense frame the debug map -- the tracker's projected depths overwritten
+    by the BP node depths -- is bit-exact with the oracle's replay, and the
+    fused depth agrees with the oracle's upsampling and fusion of it."""
+    from open_quadtree_mapping_b200.depthmap import Depthmap
+    from open_quadtree_mapping_b200.params import Params
+    W, H, n = 160, 128, 36
+    f = 460.0 * W / 752.0
+    imgs, Ts, gts = sequence(1, n, W, H)
+    p = Params(arith=ARITH_IEEE)
+    dm = Depthmap(W, H, f, W / 2.0, f, H / 2.0, semi2dense_ratio=1, params=p)
+    dm.set_semidense(True)
+    pol = PolicyReplay(num_slots=5)
+    cam = (f, f, W / 2.0, H / 2.0)
+    trk = np.zeros((H, W, 4), np.float32)
+    dep = np.zeros((H, W, 4), np.float32)
+    seeds = np.zeros((H, W, 4), np.float32)
+    n_dense = n_semi = 0
+    for i in range(n):
+        has = dm.add_frames(imgs[i], Ts[i])
+        r = pol.add(i, Ts[i])
+        assert has == (r["outcome"] in ("first", "dense")), (i, r["outcome"])
+        k = r["sd_key"]
+        debug = oracle_mod.sd_step(imgs[k] if k is not None else None, imgs[i], cam, r["sd_T"],
+                                   r["sd_mode"], trk, dep)
+        if r["outcome"] != "dense":
+            continue
+        n_dense += 1
+        slots = [imgs[q] for q in r["slots"]]
+        o = oracle_mod.extract_depth(imgs[i], slots, r["T_slots"], cam, p, sparse=debug)
+        got = dm.getDebugmap()
+        assert np.array_equal(got, o["sparse"]), i
+        n_semi += int(((debug > 0) & (got == debug)).sum())
+        dense64 = oracle_mod.upsample(o["sparse"].astype(np.float64), imgs[i], p)
+        fused, new_seeds, _, _ = oracle_mod.fuse(dense64, seeds, r["T_fuse"], cam)
+        seeds = new_seeds.astype(np.float32)
+        depth = dm.getDepthmap()
+        valid = fused > 0
+        assert (depth > 0).mean() == pytest.approx(valid.mean(), abs=2e-3)
+        both = valid & (depth > 0)
+        if both.any():
+            rel = np.abs(depth[both] - fused[both]) / fused[both]
+            assert np.percentile(rel, 99) < 1e-5, np.percentile(rel, 99)
+    assert n_dense >= 20
+    assert n_semi > 1000  # the tracker's depths reached the upsampler
+
+
+def test_batch_with_semidense_equals_single_streams(gpu):
+    from open_quadtree_mapping_b200.depthmap import BatchDepthmap
+    from open_quadtree_mapping_b200.params import Params
+    shapes = [(160, 128, 64, 5), (192, 144, 48, 3), (128, 96, 96, 7)]
+    seqs = [sequence(30 + k, 15, w, h) for k, (w, h, _, _) in enumerate(shapes)]
+    p = Params.for_range(64, 0.5, 50.0)
+    descs = [dict(width=w, height=h, fx=460.0 * w / 752.0, fy=460.0 * w / 752.0, cx=w / 2.0,
+                  cy=h / 2.0, num_hyp=d, num_slots=f) for (w, h, d, f) in shapes]
+    batch = BatchDepthmap(descs, params=p)
+    batch.set_semidense(True)
+    singles = [BatchDepthmap([d], params=p) for d in descs]
+    for s in singles:
+        s.set_semidense(True)
+    plain = BatchDepthmap(descs, params=p)
+    for i in range(15):
+        imgs = [s[0][i] for s in seqs]
+        poses = [s[1][i] for s in seqs]
+        hb = batch.add_frames(imgs, poses)
+        plain.add_frames(imgs, poses)
+        for k in range(len(shapes)):
+            assert singles[k].add_frames([imgs[k]], [poses[k]])[0] == hb[k]
+    for k in range(len(shapes)):
+        assert np.array_equal(batch.get_depth(k), singles[k].get_depth(0))
+        assert np.array_equal(batch.get_debug(k), singles[k].get_debug(0))
+        # the tracker adds depths to the debug map beyond the BP node pixels
+        assert (batch.get_debug(k) > 0).sum() > (plain.get_debug(k) > 0).sum()
+    with pytest.raises(Exception):
+        batch.set_semidense(False)  # only before the first frame
+
+
+def test_bilinear_emulation_matches_texture_unit(oracle_mod, gpu):
+    """The oracle's (and the IEEE kernels') bilinear sampling -- the texture
+    unit's formula with the fractional weights rounded to 8 bits -- against
+    the texture unit itself, set up as the reference's bindTexture does, at
+    random in-range, edge and out-of-range coordinates."""
+    from oracle import refbuild
+    if not refbuild.available():
+        pytest.skip("reference comparator not built")
+    rng = np.random.default_rng(5)
+    img = rng.integers(0, 256, (37, 53), dtype=np.uint8)
+    uv = np.concatenate([rng.uniform(-3.0, 56.0, (20000, 2)),
+                         np.floor(rng.uniform(0, 52, (2000, 2))) + rng.integers(0, 257, (2000, 2)) / 256.0,
+                         np.array([[0.5, 0.5], [53.0, 37.0], [-10.0, 5.25], [26.5, 40.0]])]
+                        ).astype(np.float32)
+    hw = refbuild.tex_sample(img, uv)
+    sw = oracle_mod.sd_sample(img, uv)
+    assert np.array_equal(hw, sw), np.abs(hw - sw).max()
