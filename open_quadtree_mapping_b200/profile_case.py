@@ -1,18 +1,19 @@
 """A small, self-contained run of the batched pipeline for profiler captures.
 
     python -m open_quadtree_mapping_b200.profile_case --streams 4 --runs 3
+    python -m open_quadtree_mapping_b200.profile_case --large --streams 2 --runs 1
 
-Feeds S synthetic 752x480 streams (64 hypotheses, 5 slots) until every
-stream produces a depth map, then replays the resident dense pipeline R more
-times.  Sized so that a kernel-level capture (ncu -k ... -c ...) stays well
-under a few GB of device memory; prints the device time per run.
+Feeds S synthetic streams (default 752x480, 64 hypotheses, 5 slots; with
+--large 1920x1080, fx=fy=1150, 128 hypotheses, 20 slots, 5-level quadtree)
+until every stream produces a depth map, then replays the resident dense
+pipeline R more times.  Sized so that a kernel-level capture (ncu -k ... -c
+...) stays well under a few GB of device memory; prints the device time per
+run.
 """
 from __future__ import annotations
 
 import argparse
 import time
-
-W, H, F = 752, 480, 460.0
 
 
 def main():
@@ -20,6 +21,8 @@ def main():
     ap.add_argument("--streams", type=int, default=4)
     ap.add_argument("--runs", type=int, default=3)
     ap.add_argument("--eager", action="store_true", help="launch stage by stage, no graph")
+    ap.add_argument("--large", action="store_true",
+                    help="1920x1080, 128 hypotheses, 20 slots, 5-level quadtree")
     args = ap.parse_args()
 
     import torch
@@ -28,10 +31,16 @@ def main():
     from .depthmap import BatchDepthmap
     from .params import Params
 
-    n_frames = 13
+    if args.large:
+        W, H, F, D, slots, n_frames = 1920, 1080, 1150.0, 128, 20, 22
+        params = Params.for_range(D, 0.5, 50.0, qt_max_level=5)
+    else:
+        W, H, F, D, slots, n_frames = 752, 480, 460.0, 64, 5, 13
+        params = Params.for_range(D, 0.5, 50.0)
     imgs, Ts, _ = synthetic.make_sequence(4000, n_frames, W=W, H=H, fx=F, fy=F)
-    desc = dict(width=W, height=H, fx=F, fy=F, cx=W / 2.0, cy=H / 2.0, num_hyp=64, num_slots=5)
-    b = BatchDepthmap([desc] * args.streams, params=Params.for_range(64, 0.5, 50.0))
+    desc = dict(width=W, height=H, fx=F, fy=F, cx=W / 2.0, cy=H / 2.0, num_hyp=D,
+                num_slots=slots)
+    b = BatchDepthmap([desc] * args.streams, params=params)
     if args.eager:
         b.set_graphs(False)
     for i in range(n_frames):

@@ -16,6 +16,8 @@ Prints one JSON line per workload (seeded synthetic ray-cast scenes):
 * diff8: 8 keyframes of 752x480 through the differentiable pipeline (soft
   readout tau=0.05, weighted upsampling, fusion, L1 loss): forward +
   backward per batch.
+* semidense32: 32 streams of 752x480 end to end with and without the
+  semi-dense tracker (its cost per stream and frame).
 
 Per-step latencies flush the L2 (a 256 MiB write) before every timed step;
 back-to-back throughput runs use working sets larger than the L2.
@@ -124,7 +126,9 @@ def _batch_workload(name, descs, seqs, layout, params, steps, warm_frames, extra
         batch.submit(*frame(cyc[j % len(cyc)]), outs=outs[j % 2])
     batch.wait()
     e2e_ms = 1000.0 * (time.perf_counter() - t0) / steps
+    prof = {k: round(v[0], 4) for k, v in batch.profile().items()}
     line = {"workload": name, "streams": S, "maps_per_s": round(S / (ms * 1e-3), 2),
+            "kernel_ms_eager": prof,
             "ms_per_step": round(ms, 4),
             "step_latency_ms": {"p50": round(_pct(lat, 50), 4), "p99": round(_pct(lat, 99), 4),
                                 "l2": "flushed before every step"},
@@ -254,8 +258,56 @@ def diff8(steps):
                       "per-pixel omega"}
 
 
+def semidense32(steps):
+    """32 streams of 752x480 (64 hypotheses, 5 slots) end to end through
+    the pipelined API with and without the semi-dense tracker; every frame
+    of every stream runs the tracker, so its cost per frame is the
+    difference."""
+    import torch
+
+    from .depthmap import BatchDepthmap
+    from .params import Params
+    W, H, f = 752, 480, 460.0
+    seqs = render_sequences([(60, W, H, f), (61, W, H, f)], 21)
+    layout = [60, 61] * 16
+    p = Params.for_range(64, 0.5, 50.0)
+    desc = dict(width=W, height=H, fx=f, fy=f, cx=W / 2.0, cy=H / 2.0, num_hyp=64, num_slots=5)
+    out = {}
+    for on in (False, True):
+        b = BatchDepthmap([desc] * 32, params=p)
+        b.set_semidense(on)
+        pinned = {}
+        for sid in (60, 61):
+            for i, img in enumerate(seqs[sid][0]):
+                t = torch.empty(img.shape, dtype=torch.uint8, pin_memory=True)
+                t.numpy()[:] = img
+                pinned[(sid, i)] = t.numpy()
+        outs = [[torch.empty((H, W), dtype=torch.float32, pin_memory=True).numpy()
+                 for _ in layout] for _ in range(2)]
+
+        def frame(i):
+            return ([pinned[(sid, i)] for sid in layout], [seqs[sid][1][i] for sid in layout])
+
+        for i in range(13):
+            b.add_frames(*frame(i))
+        for j in range(3):
+            b.submit(*frame(13 + j % 8), outs=outs[j % 2])
+        b.wait()
+        t0 = time.perf_counter()
+        for j in range(steps):
+            b.submit(*frame(13 + j % 8), outs=outs[j % 2])
+        b.wait()
+        out["on" if on else "off"] = 1000.0 * (time.perf_counter() - t0) / steps
+        b.close()
+    return {"workload": "semidense32", "streams": 32,
+            "e2e_ms_per_step": {"without_tracker": round(out["off"], 3),
+                                "with_tracker": round(out["on"], 3)},
+            "tracker_ms_per_stream_frame": round((out["on"] - out["off"]) / 32, 4),
+            "config": "32x752x480, 64 hyp, 5 slots; every step = one frame of every stream"}
+
+
 WORKLOADS = {"video720": video720, "uneven16": uneven16, "large1080": large1080,
-             "diff8": diff8}
+             "diff8": diff8, "semidense32": semidense32}
 
 
 def main():
