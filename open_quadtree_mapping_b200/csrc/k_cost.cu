@@ -4,10 +4,11 @@
 // A block owns a tile of kCostCells consecutive cells of one cell row.  Warp
 // 0 finds the tile's node cells (ballot) and stages, per node, its ray and
 // 3x3 reference patch in shared memory; the block also stages the slot poses
-// and the hypothesis depths.  The block's threads then take the (node,
-// hypothesis) pairs node-fastest, so the lanes of a warp evaluate
-// neighbouring nodes at one depth: their projections are neighbours in the
-// slot image and a gather touches few cache lines.  Each pair loops over the
+// and the hypothesis depths.  Thread t then owns node t % n (n nodes in the
+// tile) and every (256 / n)-th hypothesis from t / n on, so the lanes of a
+// warp evaluate neighbouring nodes at one depth: their projections are
+// neighbours in the slot image and a gather touches few cache lines; the
+// node's ray and patch stay in registers.  Each pair loops over the
 // measurement slots and accumulates the 3x3 SAD as an integer: every term is
 // an integer intensity difference, so the sum is exact and equal to the
 // reference's shared-memory tree over slots.  The projection follows the
@@ -62,8 +63,12 @@ __device__ __forceinline__ void patch_axis(float u, float a, float b, float (&c)
   }
 }
 
+// At most 48 registers (5 blocks of 256 threads per SM): the kernel is
+// issue-bound and gains more from resident warps than it loses to a few
+// spilled values (measured on a B200, 1920x1080 / 128 hypotheses / 20 slots:
+// 2.29 ms per 2 streams at 5 blocks, 2.65 ms at 60 registers).
 template <class A>
-__global__ void __launch_bounds__(kFlatThreads)
+__global__ void __launch_bounds__(kFlatThreads, 5)
     k_cost(const __grid_constant__ Batch B)
 {
   // costs of the tile, [kCostCells][D + 1] (the padding keeps lanes that
@@ -135,15 +140,23 @@ __global__ void __launch_bounds__(kFlatThreads)
   // are floats, the comparisons exact; NaN fails)
   const float ulo = 1.5f, uhi = (float)W - 2.5f, vhi = (float)H - 2.5f;
   const unsigned bias = 0u - kHalfBias * ((unsigned)pitch + 1u);
-  // (node, hypothesis) pairs, node fastest: lanes of a warp hold
-  // neighbouring nodes, whose projections are neighbours in the slot images
-  if (n > 0)
+  // Thread t evaluates node k = t % n at hypotheses g, g + per, g + 2 per,
+  // ... (g = t / n, per = threads per node): consecutive lanes hold
+  // neighbouring nodes at one depth, whose projections are neighbours in the
+  // slot images.  The node's ray and 3x3 patch stay in registers across the
+  // thread's hypotheses and slots.
+  const int per = n > 0 ? (int)blockDim.x / n : 0;
+  if (n > 0 && tid < per * n)
   {
-    const int step_d = blockDim.x / n, step_k = blockDim.x - step_d * n;
-    int k = tid % n, d = tid / n;
-    for (; d < D; d += step_d)
+    const int k = tid % n, g = tid / n;
+    const float3 dir = make_float3(s_dir[0][k], s_dir[1][k], s_dir[2][k]);
+    unsigned patch[9];
+#pragma unroll
+    for (int t = 0; t < 9; ++t)
+      patch[t] = (unsigned)s_patch[t][k];
+    const int col = s_col[k] * sd;
+    for (int d = g; d < D; d += per)
     {
-      const float3 dir = make_float3(s_dir[0][k], s_dir[1][k], s_dir[2][k]);
       const float3 p = A::scale(dir, s_depth[d]);
       int sad = 0, nvalid = 0;
       for (int f = 0; f < F; ++f)
@@ -173,7 +186,7 @@ __global__ void __launch_bounds__(kFlatThreads)
             const unsigned hx = twice_round_bits(px[t]) >> 1;
             const unsigned hy = twice_round_bits(py[t]) >> 1;
             const unsigned off = hy * (unsigned)pitch + hx + bias;
-            s = __usad((unsigned)s_patch[t][k], (unsigned)__ldg(m + off), s);
+            s = __usad(patch[t], (unsigned)__ldg(m + off), s);
           }
           const int wgt = s_w[f];
           sad += wgt * (int)s;
@@ -182,13 +195,7 @@ __global__ void __launch_bounds__(kFlatThreads)
       }
       const float c = nvalid > 0 ? A::sad_norm((float)sad, (float)nvalid) : 100.0f;
       const int add_num = D; // writer count of the cell (see above)
-      s_out[s_col[k] * sd + d] = A::div(c, (float)add_num);
-      k += step_k;
-      if (k >= n)
-      {
-        k -= n;
-        ++d;
-      }
+      s_out[col + d] = A::div(c, (float)add_num);
     }
   }
   __syncthreads();

@@ -341,6 +341,16 @@ __device__ float search_point(const SdJob &J, int x, int y, float2 epi, Fl<I> gr
       e5B(NAN);
   F second_best_score(1e9f), second_best_step(-1.0f);
   F pre_score(1e9f), this_score(1e9f);
+  // the sample of step s + 1 is fetched while step s is scored (sampling is
+  // a pure function of its coordinates and clamps, so the fetch past the last
+  // step is harmless)
+  auto fetch = [&](int step) {
+    const F sx = far_u + F((float)step) * dir_u, sy = far_v + F((float)step) * dir_v;
+    return sample<I>(J.inc_tex, J.inc_f, J.pitch, J.W, J.H,
+                     (float)((double)sx.v + 2.0 * (double)dir_u.v + 0.5),
+                     (float)((double)sy.v + 2.0 * (double)dir_v.v + 0.5));
+  };
+  F next = fetch(0);
   for (int step = 0; (float)step <= search_length.v && step <= kMaxSearch; step += 1)
   {
     pre_score = this_score;
@@ -348,9 +358,8 @@ __device__ float search_point(const SdJob &J, int x, int y, float2 epi, Fl<I> gr
     const F sx = far_u + F((float)step) * dir_u, sy = far_v + F((float)step) * dir_v;
     if (sx.v <= 1.0f || sx.v >= (float)(J.W - 1) || sy.v <= 1.0f || sy.v >= (float)(J.H - 1))
       break;
-    that_patch[4] = sample<I>(J.inc_tex, J.inc_f, J.pitch, J.W, J.H,
-                              (float)((double)sx.v + 2.0 * (double)dir_u.v + 0.5),
-                              (float)((double)sy.v + 2.0 * (double)dir_v.v + 0.5));
+    that_patch[4] = next;
+    next = fetch(step + 1);
     if (step % 2 == 0)
     {
       e1A = that_patch[4] - this_patch[4];
