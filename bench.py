@@ -344,6 +344,43 @@ def reference_cuda_time(imgs, Ts):
         return None
 
 
+def accuracy_vs_fp64(imgs, Ts, params):
+    """The error the throughput is measured at: one keyframe of the workload
+    (the first dense frame of stream 0) through the library's stage calls in
+    the benchmarked arithmetic, against the FP64 oracle on the same inputs:
+    relative error of the upsampled depth (p50 / p99 over valid pixels) and
+    the share of node cells whose BP label differs."""
+    import torch
+    from oracle import oracle
+    from oracle.policy import PolicyReplay
+    from open_quadtree_mapping_b200 import stages
+    pol = PolicyReplay(num_slots=SLOTS)
+    r = None
+    for i in range(WARM_FRAMES):
+        r = pol.add(i, Ts[i])
+    if r is None or r["outcome"] != "dense":
+        return None
+    i = WARM_FRAMES - 1
+    cam = (FX, FY, CX, CY)
+    slots = [imgs[k] for k in r["slots"]]
+    dev = torch.device("cuda")
+    g = stages.extract_depth(torch.from_numpy(np.ascontiguousarray(imgs[i])).to(dev),
+                             [torch.from_numpy(np.ascontiguousarray(m)).to(dev) for m in slots],
+                             r["T_slots"], cam, params)
+    oracle.set_threads(os.cpu_count() or 1)
+    o = oracle.extract_depth(imgs[i], slots, r["T_slots"], cam, params, dtype=np.float64)
+    dense, ref = g["dense"].cpu().numpy(), o["dense"]
+    ok = np.isfinite(ref) & (ref > 0) & np.isfinite(dense)
+    rel = np.abs(dense[ok] - ref[ok]) / ref[ok]
+    lab_g, lab_o = g["labels"].cpu().numpy(), o["labels"]
+    node = lab_o >= 0
+    return {"dense_rel_err_p50": float(np.percentile(rel, 50)),
+            "dense_rel_err_p99": float(np.percentile(rel, 99)),
+            "label_mismatch_frac": float((lab_g[node] != lab_o[node]).mean()),
+            "what": "stream 0's first dense keyframe, library stage calls (the benchmarked "
+                    "arithmetic) vs the FP64 oracle on the same inputs"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -510,6 +547,11 @@ def main():
         return
 
     ref_cuda = reference_cuda_time(seqs[0][0], seqs[0][1])
+    try:
+        accuracy = accuracy_vs_fp64(seqs[0][0], seqs[0][1], params)
+    except Exception as e:  # informational only
+        log("accuracy check failed:", e)
+        accuracy = None
     cpu = None
     if not args.no_cpu_baseline and world == 1:
         cpu = cpu_baseline(seqs[0][0], seqs[0][1])
@@ -537,6 +579,7 @@ def main():
         "clocks": clocks,
         "cpu_baseline": cpu,
         "reference_cuda_kernels": ref_cuda,
+        "accuracy": accuracy,
     }
     print(json.dumps(line), flush=True)
     if pg:
