@@ -191,6 +191,12 @@ int qm_batch_device_depth(qm_batch *b, int stream, const float **dev_ptr);
 int qm_batch_set_graphs(qm_batch *b, int enable);
 /* qm_depthmap_set_semidense for every stream of the batch. */
 int qm_batch_set_semidense(qm_batch *b, int enable);
+/* k = 1..4 concurrent branches of the dense pipeline over consecutive
+ * ranges of the streams that step together (the GPU fills one branch's
+ * latency-bound stages -- coarse BP levels, line solves -- with the others'
+ * work); 1 = one sequence over all of them; default 2.  Results do not
+ * depend on it. */
+int qm_batch_set_branches(qm_batch *b, int branches);
 /* L2 budget, in bytes, of a job range of the belief propagation: each BP
  * level runs over consecutive streams whose level costs and messages fit in
  * it, so the range's half-sweeps hit L2.  0 = every level over all streams

@@ -85,6 +85,7 @@ _SIGS = {
     "qm_batch_device_depth": (_I, [_P, _I, ctypes.POINTER(_P)]),
     "qm_batch_set_graphs": (_I, [_P, _I]),
     "qm_batch_set_semidense": (_I, [_P, _I]),
+    "qm_batch_set_branches": (_I, [_P, _I]),
     "qm_depthmap_set_semidense": (_I, [_P, _I]),
     "qm_batch_set_group_bytes": (_I, [_P, _S]),
     "qm_batch_set_autotune": (_I, [_P, _I]),

@@ -634,6 +634,16 @@ int qm_batch_device_depth(qm_batch *b, int stream, const float **dev_ptr)
   });
 }
 
+int qm_batch_set_branches(qm_batch *b, int branches)
+{
+  return guarded([&] {
+    require(b != nullptr && branches >= 1 && branches <= 4, "bad argument");
+    std::lock_guard<std::mutex> lock(b->set->mutex());
+    b->set->wait();
+    b->set->engine().set_branches(branches);
+  });
+}
+
 int qm_batch_set_semidense(qm_batch *b, int enable)
 {
   return guarded([&] {

@@ -116,11 +116,11 @@ struct StageTable
 // stay within `budget` bytes (at least one job per range); budget 0 = one
 // range.  Running the sweeps of a level range by range keeps that range's
 // costs and messages resident in L2 across the half-sweeps.
-std::vector<int> job_groups(const StageTable &T, int level, int L, size_t budget)
+std::vector<int> job_groups(const StageTable &T, int level, int L, size_t budget, int ja, int jb)
 {
-  std::vector<int> g{0};
+  std::vector<int> g{ja};
   size_t acc = 0;
-  for (int j = 0; j < T.n; ++j)
+  for (int j = ja; j < jb; ++j)
   {
     const size_t b = T.level_bytes.empty() ? 0 : T.level_bytes[(size_t)j * L + level];
     if (budget > 0 && j > g.back() && acc + b > budget)
@@ -130,16 +130,19 @@ std::vector<int> job_groups(const StageTable &T, int level, int L, size_t budget
     }
     acc += b;
   }
-  g.push_back(T.n);
+  g.push_back(jb);
   return g;
 }
 
-// Launches stages [first, last] of the sequence.  When `prof` is given, every
-// launch is bracketed by a pair of events recorded on `s`.  Returns the
-// number of kernel launches.
+// Launches stages [first, last] of the sequence for jobs [ja, jb) (jb < 0:
+// all).  When `prof` is given, every launch is bracketed by a pair of events
+// recorded on `s`.  Returns the number of kernel launches.
 int enqueue_range(const Batch &B, const StageTable &T, const qm_params &p, size_t group_bytes,
-                  int first, int last, cudaStream_t s, LaunchProfile *prof = nullptr)
+                  int first, int last, cudaStream_t s, LaunchProfile *prof = nullptr, int ja = 0,
+                  int jb = -1)
 {
+  if (jb < 0)
+    jb = T.n;
   const Stages st{p.bp_levels};
   const int L = p.bp_levels;
   const KParams kp = kparams(p);
@@ -176,7 +179,7 @@ int enqueue_range(const Batch &B, const StageTable &T, const qm_params &p, size_
     if (!in(stage))
       return;
     int grid = 0;
-    const Batch b = at(stage, 0, T.n, grid);
+    const Batch b = at(stage, ja, jb, grid);
     if (grid > 0)
       launch(kind, [&] { fn(b, grid); });
   };
@@ -189,7 +192,7 @@ int enqueue_range(const Batch &B, const StageTable &T, const qm_params &p, size_
   // inheritance, half-sweeps, and at level 0 the extraction)
   for (int l = L - 1; l >= 0; --l)
   {
-    const std::vector<int> groups = job_groups(T, l, L, group_bytes);
+    const std::vector<int> groups = job_groups(T, l, L, group_bytes, ja, jb);
     for (size_t gi = 0; gi + 1 < groups.size(); ++gi)
     {
       const int j0 = groups[gi], j1 = groups[gi + 1];
@@ -477,6 +480,12 @@ Engine::Engine(int device, const qm_params &p, const std::vector<Shape> &shapes)
   }
   check(cudaSetDevice(device), "cudaSetDevice");
   check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  check(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming), "cudaEventCreate");
+  for (int i = 0; i + 1 < kMaxBranches; ++i)
+  {
+    check(cudaStreamCreateWithFlags(&branch_[i], cudaStreamNonBlocking), "cudaStreamCreate");
+    check(cudaEventCreateWithFlags(&ev_join_[i], cudaEventDisableTiming), "cudaEventCreate");
+  }
   check(cudaEventCreate(&ev0_), "cudaEventCreate");
   check(cudaEventCreate(&ev1_), "cudaEventCreate");
   prepare_upsample_kernels();
@@ -593,6 +602,18 @@ Engine::~Engine()
     cudaEventDestroy(ev0_);
   if (ev1_)
     cudaEventDestroy(ev1_);
+  for (int i = 0; i + 1 < kMaxBranches; ++i)
+  {
+    if (branch_[i])
+    {
+      cudaStreamSynchronize(branch_[i]);
+      cudaStreamDestroy(branch_[i]);
+    }
+    if (ev_join_[i])
+      cudaEventDestroy(ev_join_[i]);
+  }
+  if (ev_fork_)
+    cudaEventDestroy(ev_fork_);
   if (stream_)
     cudaStreamDestroy(stream_);
 }
@@ -766,6 +787,17 @@ void Engine::tune_plan(Plan &pl)
   pl.tuned = true;
 }
 
+void Engine::set_branches(int k)
+{
+  k = std::max(1, std::min(k, kMaxBranches));
+  if (k == branches_)
+    return;
+  check(cudaSetDevice(device_), "cudaSetDevice");
+  check(cudaStreamSynchronize(stream_), "branch switch");
+  branches_ = k;
+  plans_.clear();
+}
+
 void Engine::set_autotune(bool on)
 {
   check(cudaSetDevice(device_), "cudaSetDevice");
@@ -834,7 +866,29 @@ int Engine::enqueue(Plan &pl, cudaStream_t s)
   const Batch B = upload((int)pl.active.size(), s);
   const Stages st{params_.bp_levels};
   pl.group_bytes = group_bytes_;
-  return enqueue_range(B, pl.table(), params_, group_bytes_, 0, st.count() - 1, s);
+  const int n = (int)pl.active.size();
+  const int k = std::min(branches_, n);
+  if (k < 2)
+    return enqueue_range(B, pl.table(), params_, group_bytes_, 0, st.count() - 1, s);
+  // k independent branches over consecutive ranges of the jobs (every stage
+  // is per job): the GPU fills the latency-bound stretches of one branch
+  // (coarse BP levels, line solves) with the other branches' work
+  check(cudaEventRecord(ev_fork_, s), "fork");
+  int nl = 0;
+  for (int i = 0; i < k; ++i)
+  {
+    cudaStream_t bs = i == 0 ? s : branch_[i - 1];
+    if (i > 0)
+      check(cudaStreamWaitEvent(bs, ev_fork_, 0), "fork");
+    nl += enqueue_range(B, pl.table(), params_, group_bytes_, 0, st.count() - 1, bs, nullptr,
+                        n * i / k, n * (i + 1) / k);
+  }
+  for (int i = 1; i < k; ++i)
+  {
+    check(cudaEventRecord(ev_join_[i - 1], branch_[i - 1]), "join");
+    check(cudaStreamWaitEvent(s, ev_join_[i - 1], 0), "join");
+  }
+  return nl;
 }
 
 void Engine::run(const std::vector<int> &active)

@@ -283,6 +283,11 @@ class BatchDepthmap:
         the first frame)."""
         _lib.check(_lib.lib().qm_batch_set_semidense(self._h, 1 if on else 0))
 
+    def set_branches(self, k: int) -> None:
+        """2: two concurrent pipeline branches over the two halves of the
+        streams; 1: one sequence (results are the same)."""
+        _lib.check(_lib.lib().qm_batch_set_branches(self._h, int(k)))
+
     def set_graphs(self, on: bool) -> None:
         _lib.check(_lib.lib().qm_batch_set_graphs(self._h, 1 if on else 0))
 

@@ -90,6 +90,10 @@ def test_batch_equals_plain_and_graph_equals_eager(gpu):
     split.set_group_bytes(1)
     whole = BatchDepthmap([_stream_kw()] * 3, params=p)
     whole.set_group_bytes(0)
+    # one launch sequence over all streams (the default runs two concurrent
+    # branches over the halves of the streams)
+    branched = BatchDepthmap([_stream_kw()] * 3, params=p)
+    branched.set_branches(1)
     singles = [BatchDepthmap([_stream_kw()], params=p) for _ in range(3)]
     for i in range(14):
         imgs = [s[0][i] for s in seqs]
@@ -98,6 +102,7 @@ def test_batch_equals_plain_and_graph_equals_eager(gpu):
         he = eager.add_frames(imgs, poses)
         assert split.add_frames(imgs, poses) == hb
         assert whole.add_frames(imgs, poses) == hb
+        assert branched.add_frames(imgs, poses) == hb
         hs = [singles[k].add_frames([imgs[k]], [poses[k]])[0] for k in range(3)]
         assert hb == he == hs
         if all(hb) and i > 0:
@@ -108,6 +113,7 @@ def test_batch_equals_plain_and_graph_equals_eager(gpu):
                 assert np.array_equal(a, eager.get_depth(k))
                 assert np.array_equal(a, split.get_depth(k))
                 assert np.array_equal(a, whole.get_depth(k))
+                assert np.array_equal(a, branched.get_depth(k))
                 assert np.array_equal(a, singles[k].get_depth(0))
                 assert np.array_equal(batch.get_debug(k), singles[k].get_debug(0))
     assert batch.last_launches() > 0
