@@ -486,8 +486,11 @@ __device__ float search_point(const SdJob &J, int x, int y, float2 epi, Fl<I> gr
 
 // update_keyframe_kernel (lsd_semidense.cu:400-515): one stereo observation
 // per seed; reads and writes only its own seed.
+// 3 blocks per SM (at most 85 registers instead of 86 / 102, i.e. 2 blocks):
+// the search loop is latency-bound, and the third block's warps outweigh the
+// few spilled values
 template <bool I>
-__global__ void __launch_bounds__(kSdThreads) k_sd_update(const __grid_constant__ SdBatch B)
+__global__ void __launch_bounds__(kSdThreads, 3) k_sd_update(const __grid_constant__ SdBatch B)
 {
   using F = Fl<I>;
   int lb, x, y;

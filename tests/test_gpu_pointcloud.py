@@ -80,3 +80,26 @@ def test_facade_point_cloud(oracle_mod, gpu):
             assert _same(batch.get_point_cloud(1), want)
             n_points.append(len(got))
     assert max(n_points) > 0  # fused depth became valid somewhere
+
+
+def test_point_cloud_rejects_small_workspace(gpu):
+    import ctypes
+    from open_quadtree_mapping_b200 import _lib
+    H, W = 48, 64
+    depth = torch.ones((H, W), dtype=torch.float32, device=gpu)
+    ref = torch.zeros((H, W), dtype=torch.uint8, device=gpu)
+    pts = torch.empty((H * W, 4), dtype=torch.float32, device=gpu)
+    count = torch.zeros(1, dtype=torch.int32, device=gpu)
+    need = ctypes.c_size_t()
+    _lib.check(_lib.lib().qm_point_cloud_workspace_size(W, H, ctypes.byref(need)))
+    ws = torch.empty(need.value, dtype=torch.uint8, device=gpu)
+    c = _lib.QmCamera(50.0, 50.0, 32.0, 24.0)
+    T = np.ascontiguousarray(np.eye(3, 4, dtype=np.float32).reshape(12))
+    st = _lib.lib().qm_point_cloud(depth.data_ptr(), W, ref.data_ptr(), W, W, H, ctypes.byref(c),
+                                   T.ctypes.data, pts.data_ptr(), count.data_ptr(), ws.data_ptr(),
+                                   need.value - 1, None)
+    assert st != 0
+    st = _lib.lib().qm_point_cloud(depth.data_ptr(), W - 1, ref.data_ptr(), W, W, H,
+                                   ctypes.byref(c), T.ctypes.data, pts.data_ptr(),
+                                   count.data_ptr(), ws.data_ptr(), need.value, None)
+    assert st != 0  # depth stride below the width

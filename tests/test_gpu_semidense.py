@@ -213,3 +213,36 @@ def test_reference_arith_tracks_the_reference_kernels(gpu):
         # measured by frame 23: 79 % overlap, median 2e-3 (two runs of the
         # reference itself: 93 %, 2e-5)
         assert overlap > 0.7 and rel < 5e-3, (i, overlap, rel)
+
+
+def test_semidense_step_rejects_bad_arguments(gpu):
+    import ctypes
+    from open_quadtree_mapping_b200 import _lib, stages
+    H, W = 64, 80
+    inc = torch.zeros((H, W), dtype=torch.uint8, device=gpu)
+    trk = torch.zeros((H, W, 4), dtype=torch.float32, device=gpu)
+    dep = torch.zeros((H, W, 4), dtype=torch.float32, device=gpu)
+    cam = (60.0, 60.0, W / 2.0, H / 2.0)
+    T = np.eye(3, 4, dtype=np.float32)
+    with pytest.raises(_lib.QmError):
+        stages.semidense_step(inc, inc, cam, T, 7, trk, dep)  # no such mode
+    with pytest.raises(_lib.QmError):
+        stages.semidense_step(None, inc, cam, T, stages.SD_UPDATE, trk, dep)  # no keyframe
+    with pytest.raises(_lib.QmError):
+        stages.semidense_step(inc, inc, cam, T, stages.SD_UPDATE, trk, dep, arith=5)
+    # a workspace one byte short is refused before anything runs
+    need = ctypes.c_size_t()
+    _lib.check(_lib.lib().qm_semidense_workspace_size(W, H, ctypes.byref(need)))
+    ws = torch.empty(need.value, dtype=torch.uint8, device=gpu)
+    debug = torch.empty((H, W), dtype=torch.float32, device=gpu)
+    c = _lib.QmCamera(*cam)
+    T12 = np.ascontiguousarray(T.reshape(12))
+    st = _lib.lib().qm_semidense_step(None, inc.data_ptr(), W, H, ctypes.byref(c),
+                                      T12.ctypes.data, stages.SD_INIT, 0, trk.data_ptr(),
+                                      dep.data_ptr(), debug.data_ptr(), ws.data_ptr(),
+                                      need.value - 1, None)
+    assert st != 0
+    # and with the right size the first-frame step runs
+    stages.semidense_step(None, inc, cam, T, stages.SD_INIT, trk, dep)
+    torch.cuda.synchronize()
+    assert float(trk[..., 0].max()) == 0.0  # a flat image has no gradient: no seeds
