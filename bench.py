@@ -499,9 +499,12 @@ def main():
 
     # ---- per-kernel profile (eager launches with events) for the roofline
     prof = batch.profile()
-    from oracle import oracle
-    levels_list = [oracle.quadtree(seqs[s % len(seqs)][0][WARM_FRAMES - 1], params)
-                   for s in range(S)]
+    # the quadtree levels of the profiled frames (for the cells the BP
+    # actually updates), from the library's own quadtree kernel
+    from open_quadtree_mapping_b200 import stages
+    lv_by_seq = {k: stages.quadtree(torch.from_numpy(np.ascontiguousarray(
+        seqs[k][0][WARM_FRAMES - 1])).cuda(), params).cpu().numpy() for k in range(len(seqs))}
+    levels_list = [lv_by_seq[s % len(seqs)] for s in range(S)]
     alg = algorithmic_bytes(levels_list, params)
     peak, peak_kind = measured_hbm_peak()
     kinds = {}
@@ -546,15 +549,18 @@ def main():
             pg.destroy_process_group()
         return
 
-    ref_cuda = reference_cuda_time(seqs[0][0], seqs[0][1])
-    try:
-        accuracy = accuracy_vs_fp64(seqs[0][0], seqs[0][1], params)
-    except Exception as e:  # informational only
-        log("accuracy check failed:", e)
-        accuracy = None
-    cpu = None
+    # ---- the baseline leg (rank 0 at N=1 only): the CPU port of the
+    # reference on the host cores, the reference's own kernels on this GPU,
+    # and the error this run's arithmetic is measured at against the FP64
+    # oracle
+    cpu = ref_cuda = accuracy = None
     if not args.no_cpu_baseline and world == 1:
         cpu = cpu_baseline(seqs[0][0], seqs[0][1])
+        ref_cuda = reference_cuda_time(seqs[0][0], seqs[0][1])
+        try:
+            accuracy = accuracy_vs_fp64(seqs[0][0], seqs[0][1], params)
+        except Exception as e:  # informational only
+            log("accuracy check failed:", e)
 
     value = S * world / (ms_step * 1e-3)
     line = {

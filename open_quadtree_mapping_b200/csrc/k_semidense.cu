@@ -486,11 +486,12 @@ __device__ float search_point(const SdJob &J, int x, int y, float2 epi, Fl<I> gr
 
 // update_keyframe_kernel (lsd_semidense.cu:400-515): one stereo observation
 // per seed; reads and writes only its own seed.
-// 3 blocks per SM (at most 85 registers instead of 86 / 102, i.e. 2 blocks):
-// the search loop is latency-bound, and the third block's warps outweigh the
-// few spilled values
+// 4 blocks per SM (at most 64 registers instead of 86 / 102, i.e. 2 blocks):
+// the search loop is latency-bound, and the extra resident warps outweigh
+// the spilled values (tracker per stream and frame at 752x480: 0.171 ms at
+// 2 blocks, 0.144 at 3, 0.127 at 4, 0.125 at 5)
 template <bool I>
-__global__ void __launch_bounds__(kSdThreads, 3) k_sd_update(const __grid_constant__ SdBatch B)
+__global__ void __launch_bounds__(kSdThreads, 4) k_sd_update(const __grid_constant__ SdBatch B)
 {
   using F = Fl<I>;
   int lb, x, y;
