@@ -1,6 +1,6 @@
 """Algorithm parameters of the depth pipeline, with the reference's values.
 
-The reference compiles every constant in (SURVEY of stereo_parameter.cuh:2-42,
+The reference compiles every constant in (stereo_parameter.cuh:2-42,
 pixel_cost.cuh:4, bpextract.cu:41-45,222-223, quadtree.cu:40,59,74,
 depth_upsample.cu, depth_fusion.cu:13-15).  Here they are one runtime struct,
 `qm_params` in include/qm_capi.h; this module mirrors it for Python callers.
