@@ -197,10 +197,13 @@ def algorithmic_bytes(levels_list, params):
         for l in range(1, params.bp_levels):
             by["pyramid"] += 4 * D * (sizes[l - 1] + sizes[l])
         # message inheritance writes the four messages of the cells the
-        # quadtree test skips (copied from the parent level, zeros at the top)
+        # quadtree test skips (copied from the parent level, zeros at the
+        # top); at a level with two or more half-sweeps the first two sweeps
+        # write them, otherwise a separate pass does
         for l, (w, h, counts) in enumerate(cells):
             skipped = w * h - counts[0] - counts[1]
-            by["msg_init"] += 16 * D * skipped * (2 if l + 1 < params.bp_levels else 1)
+            kind = "bp_sweep" if params.bp_iters[l] >= 2 else "msg_init"
+            by[kind] += 16 * D * skipped * (2 if l + 1 < params.bp_levels else 1)
         for l, (w, h, counts) in enumerate(cells):
             it = params.bp_iters[l]
             n = sum(counts[i & 1] for i in range(it))

@@ -197,7 +197,10 @@ int enqueue_range(const Batch &B, const StageTable &T, const qm_params &p, size_
     {
       const int j0 = groups[gi], j1 = groups[gi + 1];
       int grid = 0;
-      if (in(st.inherit(l)))
+      // with two or more half-sweeps the first two write the inherited
+      // messages themselves (no separate pass)
+      const bool fold = p.bp_iters[l] >= 2;
+      if (!fold && in(st.inherit(l)))
       {
         const Batch b = at(st.inherit(l), j0, j1, grid);
         if (grid > 0)
@@ -212,7 +215,8 @@ int enqueue_range(const Batch &B, const StageTable &T, const qm_params &p, size_
           for (int it = 0; it < p.bp_iters[l]; ++it)
             for (int d : T.dvals)
               launch(kSweep, [&] {
-                launch_bp_sweep(b, grid, d, l, it, kp, ar, s, T.tune.sweep_warps);
+                launch_bp_sweep(b, grid, d, l, it, kp, ar, s, T.tune.sweep_warps,
+                                fold && in(st.inherit(l)) ? 1 : 0);
               });
       }
       if (l == 0 && in(st.extract()))

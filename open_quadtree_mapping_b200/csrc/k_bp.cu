@@ -225,7 +225,9 @@ __device__ __forceinline__ bool bp_skipped(const JobDesc &J, int level, int x, i
 // kernel's `first` mode), and every cell the sweeps update overwrites its
 // copy before anyone reads it.  The copies that ARE read later are written
 // here: cells the quadtree test skips at this level, and, with fewer than two
-// iterations, the cells no sweep reaches.
+// iterations, the cells no sweep reaches.  With two or more iterations the
+// batched pipeline does not launch this pass: half-sweeps 0 and 1 copy the
+// skipped cells of their own colour (the sweep kernel's `inherit` mode).
 __global__ void __launch_bounds__(kFlatThreads)
     k_msg_inherit(const __grid_constant__ Batch B, int level, int iters, int qt_max)
 {
@@ -266,7 +268,8 @@ __global__ void __launch_bounds__(kFlatThreads)
 // the warp's shuffles (full masks) with zero inputs and store nothing.
 template <int D, int ARITH>
 __global__ void __launch_bounds__(kMaxCellWarps * 32, 4)
-    k_bp_sweep(const __grid_constant__ Batch B, int level, int parity, int first, KParams kp)
+    k_bp_sweep(const __grid_constant__ Batch B, int level, int parity, int first, int inherit,
+               KParams kp)
 {
   using HL = HypLayout<D>;
   constexpr int NV = HL::NV, LPC = HL::LPC, G = HL::G;
@@ -282,12 +285,33 @@ __global__ void __launch_bounds__(kMaxCellWarps * 32, 4)
     return; // the whole warp
   const int item = item0 + lane / LPC;
   int x = 0, y = 0;
-  bool act = item < hw * h;
+  bool act = item < hw * h, skipped = false;
   if (act)
   {
     y = item / hw;
     x = 2 * (item - y * hw) + ((y + parity) & 1); // item - y*hw == x / 2
-    act = x < w && !bp_skipped(J, level, x, y, kp.qt_max);
+    skipped = x < w && bp_skipped(J, level, x, y, kp.qt_max);
+    act = x < w && !skipped;
+  }
+  if (inherit && skipped)
+  {
+    // message inheritance of a cell the quadtree test skips at this level:
+    // its messages keep the parent's (zeros at the coarsest level), as the
+    // reference's copied-down images hold them (bpextract.cu:87-90,374-395);
+    // half-sweeps 0 and 1 write them for their colour before any later
+    // half-sweep reads them
+    const size_t c = (size_t)y * w + x;
+    const bool top = level + 1 >= J.nlev;
+    const LevelDesc &C = J.lv[top ? level : level + 1];
+    const size_t pc = ((size_t)(y >> 1) * C.w + (x >> 1)) * D;
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+#pragma unroll
+      for (int k = 0; k < NV; ++k)
+      {
+        const int d = gl + LPC * k;
+        L.msg[m][c * D + d] = top ? 0.0f : C.msg[m][pc + d];
+      }
   }
   if (!__any_sync(0xffffffffu, act))
     return;
@@ -498,13 +522,15 @@ __global__ void __launch_bounds__(kMaxCellWarps * 32)
 }
 
 template <int D>
-void sweep_d(const Batch &B, int blocks, int level, int parity, int first, KParams kp,
-             int arith, int warps, cudaStream_t s)
+void sweep_d(const Batch &B, int blocks, int level, int parity, int first, int inherit,
+             KParams kp, int arith, int warps, cudaStream_t s)
 {
   if (arith == QM_ARITH_IEEE)
-    k_bp_sweep<D, QM_ARITH_IEEE><<<blocks, warps * 32, 0, s>>>(B, level, parity, first, kp);
+    k_bp_sweep<D, QM_ARITH_IEEE>
+        <<<blocks, warps * 32, 0, s>>>(B, level, parity, first, inherit, kp);
   else
-    k_bp_sweep<D, QM_ARITH_REFERENCE><<<blocks, warps * 32, 0, s>>>(B, level, parity, first, kp);
+    k_bp_sweep<D, QM_ARITH_REFERENCE>
+        <<<blocks, warps * 32, 0, s>>>(B, level, parity, first, inherit, kp);
 }
 
 template <int D>
@@ -549,31 +575,32 @@ void launch_msg_inherit(const Batch &B, int blocks, int level, int iters, int qt
 // each launch skips the jobs of other counts.
 namespace
 {
-void sweep_any(const Batch &B, int blocks, int d, int level, int parity, int first, KParams kp,
-               int arith, int warps, cudaStream_t s)
+void sweep_any(const Batch &B, int blocks, int d, int level, int parity, int first, int inherit,
+               KParams kp, int arith, int warps, cudaStream_t s)
 {
   switch (d)
   {
-  case 32: sweep_d<32>(B, blocks, level, parity, first, kp, arith, warps, s); break;
-  case 48: sweep_d<48>(B, blocks, level, parity, first, kp, arith, warps, s); break;
-  case 64: sweep_d<64>(B, blocks, level, parity, first, kp, arith, warps, s); break;
-  case 96: sweep_d<96>(B, blocks, level, parity, first, kp, arith, warps, s); break;
-  case 128: sweep_d<128>(B, blocks, level, parity, first, kp, arith, warps, s); break;
+  case 32: sweep_d<32>(B, blocks, level, parity, first, inherit, kp, arith, warps, s); break;
+  case 48: sweep_d<48>(B, blocks, level, parity, first, inherit, kp, arith, warps, s); break;
+  case 64: sweep_d<64>(B, blocks, level, parity, first, inherit, kp, arith, warps, s); break;
+  case 96: sweep_d<96>(B, blocks, level, parity, first, inherit, kp, arith, warps, s); break;
+  case 128: sweep_d<128>(B, blocks, level, parity, first, inherit, kp, arith, warps, s); break;
   default: break;
   }
 }
 } // namespace
 
 void launch_bp_sweep(const Batch &B, int blocks, int d, int level, int it, KParams kp, int arith,
-                     cudaStream_t s, int warps)
+                     cudaStream_t s, int warps, int inherit)
 {
-  sweep_any(B, blocks, d, level, it & 1, it == 0 ? 1 : 0, kp, arith, warps, s);
+  sweep_any(B, blocks, d, level, it & 1, it == 0 ? 1 : 0, inherit && it < 2 ? 1 : 0, kp, arith,
+            warps, s);
 }
 
 void launch_bp_sweep_own(const Batch &B, int blocks, int d, int level, int parity, KParams kp,
                          int arith, cudaStream_t s, int warps)
 {
-  sweep_any(B, blocks, d, level, parity, 0, kp, arith, warps, s);
+  sweep_any(B, blocks, d, level, parity, 0, 0, kp, arith, warps, s);
 }
 
 void launch_extract(const Batch &B, int blocks, int d, int arith, cudaStream_t s, int warps)

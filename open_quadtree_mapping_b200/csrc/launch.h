@@ -59,9 +59,12 @@ void launch_pyramid(const Batch &B, int blocks, int level, cudaStream_t s);
 // (cells the quadtree test skips; all unswept cells when iters < 2)
 void launch_msg_inherit(const Batch &B, int blocks, int level, int iters, int qt_max,
                         cudaStream_t s);
-// half-sweep `it` (0-based) of level `level`; `warps` per block
+// half-sweep `it` (0-based) of level `level`; `warps` per block.  inherit:
+// half-sweeps 0 and 1 also write the inherited messages of their colour's
+// cells the quadtree test skips (instead of launch_msg_inherit; the level
+// must have at least two half-sweeps)
 void launch_bp_sweep(const Batch &B, int blocks, int d, int level, int it, KParams kp, int arith,
-                     cudaStream_t s, int warps = kCellWarps);
+                     cudaStream_t s, int warps = kCellWarps, int inherit = 0);
 // a half-sweep of colour `parity` that reads every incoming message from the
 // level's own buffers (all cells' starting messages already written)
 void launch_bp_sweep_own(const Batch &B, int blocks, int d, int level, int parity, KParams kp,
