@@ -191,7 +191,8 @@ def algorithmic_bytes(levels_list, params):
                            "fuse_update")}
     for lv in levels_list:
         cells = bp_updated_cells(lv, params)
-        by["quadtree"] += 2 * P
+        # levels written, the debug depth cleared
+        by["quadtree"] += P * (1 + 4) + P
         by["cost"] += P * (1 + SLOTS) + C + 4 * C * D
         sizes = [(w * h) for (w, h, _) in cells]
         for l in range(1, params.bp_levels):
@@ -209,12 +210,14 @@ def algorithmic_bytes(levels_list, params):
             n = sum(counts[i & 1] for i in range(it))
             by["bp_sweep"] += 36 * D * n
         by["extract"] += C * (20 * D + 4)
-        # both solves derive the smoothness weights from the image in-kernel
-        by["row_solve"] += P * (4 + 1 + 8)
+        # both solves derive the smoothness weights from the image in-kernel;
+        # the row solve also resets the fusion keys
+        by["row_solve"] += P * (4 + 1 + 8 + 8)
         by["col_solve"] += P * (8 + 1 + 4)
         by["fuse_transform"] += P * 32
-        by["fuse_fill"] += P * 12
-        by["fuse_update"] += P * 52
+        # hole filling runs inside the update: depth, key and source seed
+        # read, depth and seed written
+        by["fuse_update"] += P * (4 + 8 + 16 + 4 + 16)
     return by
 
 

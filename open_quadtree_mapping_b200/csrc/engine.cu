@@ -45,9 +45,8 @@ struct Stages
   int row() const { return 2 + 3 * L; }
   int col() const { return 3 + 3 * L; }
   int ftrans() const { return 4 + 3 * L; }
-  int ffill() const { return 5 + 3 * L; }
-  int fupd() const { return 6 + 3 * L; }
-  int count() const { return 7 + 3 * L; }
+  int fupd() const { return 5 + 3 * L; } // hole filling + posterior update
+  int count() const { return 6 + 3 * L; }
 };
 
 std::vector<int> stage_blocks(const Shape &s, const JobLayout &lay, const qm_params &p,
@@ -72,7 +71,7 @@ std::vector<int> stage_blocks(const Shape &s, const JobLayout &lay, const qm_par
   b[st.extract()] = cdiv((long)lay.lw[0] * lay.lh[0], epb);
   b[st.row()] = cdiv(s.H, tune.row_warps);
   b[st.col()] = cdiv(s.W, tune.col_lines);
-  b[st.ftrans()] = b[st.ffill()] = b[st.fupd()] = cdiv((long)s.W * s.H, kFlatThreads);
+  b[st.ftrans()] = b[st.fupd()] = cdiv((long)s.W * s.H, kFlatThreads);
   return b;
 }
 
@@ -236,7 +235,6 @@ int enqueue_range(const Batch &B, const StageTable &T, const qm_params &p, size_
   });
   all(kFuseTransform, st.ftrans(),
       [&](const Batch &b, int g) { launch_fuse_transform(b, g, ar, s); });
-  all(kFuseFill, st.ffill(), [&](const Batch &b, int g) { launch_fuse_fill(b, g, s); });
   all(kFuseUpdate, st.fupd(), [&](const Batch &b, int g) { launch_fuse_update(b, g, s); });
   check(cudaGetLastError(), "kernel launch");
   return n;
@@ -375,7 +373,7 @@ JobLayout JobLayout::make(const Shape &s, int nlev)
   L.off_seeds[0] = take(P * sizeof(float4));
   L.off_seeds[1] = take(P * sizeof(float4));
   L.off_zkey = take(P * sizeof(unsigned long long));
-  L.off_table = take(P * sizeof(int32_t));
+  L.off_sdkey = take(P * sizeof(unsigned long long));
   L.bytes = o;
   return L;
 }
@@ -413,7 +411,7 @@ JobDesc make_job_desc(const Shape &s, const qm_params &p, const JobBuffers &b, i
   J.seeds_in = b.seeds[seeds_cur];
   J.seeds_out = b.seeds[seeds_cur ^ 1];
   J.zkey = b.zkey;
-  J.table = b.table;
+  J.table = nullptr; // the batched pipeline does not keep the fusion's source table
   for (int k = 0; k < 12; ++k)
     J.Tf[k] = (k == 0 || k == 5 || k == 10) ? 1.0f : 0.0f;
   return J;
@@ -530,15 +528,15 @@ Engine::Engine(int device, const qm_params &p, const std::vector<Shape> &shapes)
     B.seeds[0] = (float4 *)(b0 + L.off_seeds[0]);
     B.seeds[1] = (float4 *)(b0 + L.off_seeds[1]);
     B.zkey = (unsigned long long *)(b0 + L.off_zkey);
-    B.table = (int32_t *)(b0 + L.off_table);
+    B.sdkey = (unsigned long long *)(b0 + L.off_sdkey);
     const size_t P = (size_t)shapes[j].W * shapes[j].H;
     check(cudaMemsetAsync(B.seeds[0], 0, P * sizeof(float4) * 1, stream_), "memset");
     check(cudaMemsetAsync(B.seeds[1], 0, P * sizeof(float4) * 1, stream_), "memset");
     check(cudaMemsetAsync(B.zkey, 0xff, P * sizeof(unsigned long long), stream_), "memset");
+    check(cudaMemsetAsync(B.sdkey, 0xff, P * sizeof(unsigned long long), stream_), "memset");
     check(cudaMemsetAsync(B.sparse, 0, P * sizeof(float), stream_), "memset");
     check(cudaMemsetAsync(B.dense[0], 0, P * sizeof(float), stream_), "memset");
     check(cudaMemsetAsync(B.dense[1], 0, P * sizeof(float), stream_), "memset");
-    check(cudaMemsetAsync(B.table, 0, P * sizeof(int32_t), stream_), "memset");
   }
   slot_base_.resize(n);
   for (int j = 0; j < n; ++j)

@@ -91,8 +91,8 @@ struct JobBuffers
                         // back while the next step runs)
   float2 *rowres = nullptr;
   float4 *seeds[2] = {};
-  unsigned long long *zkey = nullptr;
-  int32_t *table = nullptr;
+  unsigned long long *zkey = nullptr;  // fusion z-buffer (reset by the row solve)
+  unsigned long long *sdkey = nullptr; // semi-dense z-buffer (all ones between its steps)
 };
 
 // Byte layout of one job's buffers (offsets from a 256-byte aligned base).
@@ -100,7 +100,7 @@ struct JobLayout
 {
   size_t bytes = 0;
   size_t off_levels, off_data[kMaxLevels], off_msg[kMaxLevels][4], off_labels, off_sparse,
-      off_dense[2], off_rowres, off_seeds[2], off_zkey, off_table;
+      off_dense[2], off_rowres, off_seeds[2], off_zkey, off_sdkey;
   int lw[kMaxLevels], lh[kMaxLevels];
   static JobLayout make(const Shape &s, int nlev);
 };

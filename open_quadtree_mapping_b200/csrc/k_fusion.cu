@@ -11,14 +11,19 @@
 //    depths are positive floats, so the key orders by depth, then by index;
 //  * hole filling reads the resolved keys: an empty pixel takes the nearest
 //    (smallest key) non-empty 3x3 neighbour among the pixels that propagate
-//    (x in [2, W-1), y in [2, H-1)); one pass, no chains.
+//    (x in [2, W-1), y in [2, H-1)); one pass, no chains.  It runs inside
+//    the update kernel (each pixel resolves its own source, then updates).
+
 // Index 0 is the "empty" table value, so pixel (0, 0) never propagates
 // (as in the reference).  The posterior update (fuse_currentmap) runs in FP64;
 // the emitted depth is mu' when the PRIOR inlier ratio a/(a+b) > 0.6, else -1.
-// The last kernel resets the z-buffer keys for the next frame.
+// The update kernel leaves the keys set (its neighbours may still read them);
+// the batched pipeline's row solve resets them in the stream's next dense
+// frame (before its transform), the stage entry point clears its workspace.
 //
-// Bytes per pixel: transform 16 read + 16 written (+ 8-byte atomic), fill
-// 9*8 read (cached) + 4 written, update 4 + 4 + 16 read, 4 + 16 + 8 written.
+// Bytes per pixel: transform 16 read + 16 written (+ 8-byte atomic); update
+// 4 + 8 + 16 read (+ the 3x3 keys of an empty pixel, cached), 4 + 16
+// written (+ 4 when the source table is kept).
 #include "launch.h"
 
 namespace qm
@@ -73,7 +78,7 @@ __global__ void __launch_bounds__(kFlatThreads)
 }
 
 __global__ void __launch_bounds__(kFlatThreads)
-    k_fuse_fill(const __grid_constant__ Batch B)
+    k_fuse_update(const __grid_constant__ Batch B)
 {
   int lb;
   const JobDesc &J = job_of(B, lb);
@@ -81,6 +86,13 @@ __global__ void __launch_bounds__(kFlatThreads)
   const int idx = lb * blockDim.x + threadIdx.x;
   if (idx >= W * H)
     return;
+  const double dep = (double)J.dense[idx];
+  double unc = fmax(0.5, dep * 0.2);
+  unc *= unc;
+  if (dep <= 0.0)
+    unc = 1e9;
+  // hole filling (hole_filling, depth_fusion.cu:121-144): the pixel's own key, or
+  // for an empty pixel the smallest key of its propagating 3x3 neighbours
   const int x = idx % W, y = idx / W;
   unsigned long long key = J.zkey[idx];
   if (key == kEmpty)
@@ -95,24 +107,9 @@ __global__ void __launch_bounds__(kFlatThreads)
         key = k < key ? k : key;
       }
   }
-  J.table[idx] = key == kEmpty ? 0 : (int)(unsigned)(key & 0xffffffffull);
-}
-
-__global__ void __launch_bounds__(kFlatThreads)
-    k_fuse_update(const __grid_constant__ Batch B)
-{
-  int lb;
-  const JobDesc &J = job_of(B, lb);
-  const int W = J.W, H = J.H;
-  const int idx = lb * blockDim.x + threadIdx.x;
-  if (idx >= W * H)
-    return;
-  const double dep = (double)J.dense[idx];
-  double unc = fmax(0.5, dep * 0.2);
-  unc *= unc;
-  if (dep <= 0.0)
-    unc = 1e9;
-  const int pre = J.table[idx];
+  const int pre = key == kEmpty ? 0 : (int)(unsigned)(key & 0xffffffffull);
+  if (J.table)
+    J.table[idx] = pre;
   double a, b, mu, s2;
   if (pre > 0)
   {
@@ -163,7 +160,6 @@ __global__ void __launch_bounds__(kFlatThreads)
   const double b_p = a_p * (1.0 - f) * inv_f;
   J.dense[idx] = (ratio > 0.60) ? (float)mu_p : -1.0f;
   J.seeds_out[idx] = make_float4((float)a_p, (float)b_p, (float)mu_p, (float)s2_p);
-  J.zkey[idx] = kEmpty;
 }
 
 // sigma^2 of every seed (the fused variance)
@@ -190,11 +186,6 @@ void launch_fuse_transform(const Batch &B, int blocks, int arith, cudaStream_t s
     k_fuse_transform<ArithIeee><<<blocks, kFlatThreads, 0, s>>>(B);
   else
     k_fuse_transform<ArithRef><<<blocks, kFlatThreads, 0, s>>>(B);
-}
-
-void launch_fuse_fill(const Batch &B, int blocks, cudaStream_t s)
-{
-  k_fuse_fill<<<blocks, kFlatThreads, 0, s>>>(B);
 }
 
 void launch_fuse_update(const Batch &B, int blocks, cudaStream_t s)

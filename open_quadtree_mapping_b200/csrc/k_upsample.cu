@@ -258,9 +258,15 @@ __global__ void __launch_bounds__(kMaxRowWarps * 32)
   LineBuf b = line_buf(smem + warp * kArrays * line_floats(max_n), n);
   const uint8_t *img = J.ref + (size_t)y * J.ref_pitch;
   const float *sp = J.sparse + (size_t)y * W;
+  // the row's fusion z-buffer keys start empty for this frame's fusion (the
+  // previous frame's update left them set); coalesced stores in a
+  // latency-bound pass
+  unsigned long long *zk = J.zkey ? J.zkey + (size_t)y * W : nullptr;
   for (int k = lane; k < n; k += 32)
   {
     const int p = b.pos(k);
+    if (zk)
+      zk[k] = ~0ull;
     const float I = (float)img[k];
     b.w[p] = k == 0 ? 0.0f : edge_weight<A>(I, (float)img[k - 1], kp.up_sigma);
     const float d = sp[k];

@@ -76,7 +76,8 @@ void launch_row_solve(const Batch &B, int blocks, KParams kp, int arith, int max
 void launch_col_solve(const Batch &B, int blocks, KParams kp, int arith, int max_h,
                       cudaStream_t s, int lines = kColLines);
 void launch_fuse_transform(const Batch &B, int blocks, int arith, cudaStream_t s);
-void launch_fuse_fill(const Batch &B, int blocks, cudaStream_t s);
+// hole filling + posterior update (reads the z-buffer keys, leaves them set:
+// the next frame's row solve resets them)
 void launch_fuse_update(const Batch &B, int blocks, cudaStream_t s);
 // out[i] = seeds[i].w (the fused variance sigma^2), n pixels
 void launch_seed_variance(const float4 *seeds, float *out, long n, cudaStream_t s);

@@ -67,7 +67,8 @@ struct JobDesc
   float2 *rowres;  // W*H row-smoothed (depth, indicator)
   float4 *seeds_in;
   float4 *seeds_out;
-  unsigned long long *zkey; // W*H z-buffer keys (all ones = empty)
+  unsigned long long *zkey; // W*H z-buffer keys (all ones = empty; the row
+                            // solve resets them when non-null)
   int32_t *table;           // W*H fusion source index (0 = none)
   float Tf[12];             // T_income<-lastfuse
   int keep_sparse;          // 1: `sparse` already holds this frame's

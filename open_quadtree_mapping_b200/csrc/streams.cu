@@ -261,7 +261,7 @@ void StreamSet::semidense_step(const std::vector<int> &which, int parity)
     }
     J.cur = 0;
     J.debug = eng_->buffers(i).sparse;
-    J.zkey = eng_->buffers(i).zkey;
+    J.zkey = eng_->buffers(i).sdkey;
     std::memcpy(J.T, s.sd_T.d, sizeof(J.T));
     prefix[n + 1] = prefix[n] + sd_blocks(s.d.W, s.d.H);
     ++n;
