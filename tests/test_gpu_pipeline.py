@@ -192,3 +192,31 @@ def test_semi2dense_ratio_and_resident_errors(gpu):
             assert not f
     with pytest.raises(_lib.QmError):
         BatchDepthmap([_stream_kw(W=100)], params=Params())
+
+
+@pytest.mark.parametrize("iters", [(1, 0, 3, 2), (2, 1, 0, 5)])
+def test_short_bp_iterations_match_oracle(oracle_mod, gpu, iters):
+    """Levels with fewer than two half-sweeps take the separate
+    message-inheritance pass, levels with two or more let their first two
+    half-sweeps write the inherited messages: with counts of 0, 1, 2, 3 and
+    5 across the levels the batched pipeline's node depths (the debug map)
+    stay bit-exact with the oracle in IEEE mode."""
+    from open_quadtree_mapping_b200.depthmap import Depthmap
+    n_frames = 15
+    imgs, Ts, _ = sequence(2, n_frames, W, H)
+    p = Params(arith=ARITH_IEEE, bp_iters=iters)
+    dm = Depthmap(W, H, F_PX, W / 2.0, F_PX, H / 2.0, semi2dense_ratio=1, params=p)
+    pol = PolicyReplay(num_slots=5)
+    cam = (F_PX, F_PX, W / 2.0, H / 2.0)
+    n_dense = 0
+    for i in range(n_frames):
+        has = dm.add_frames(imgs[i], Ts[i])
+        r = pol.add(i, Ts[i])
+        assert has == (r["outcome"] in ("first", "dense")), (i, r["outcome"])
+        if r["outcome"] != "dense":
+            continue
+        n_dense += 1
+        slots = [imgs[k] for k in r["slots"]]
+        o = oracle_mod.extract_depth(imgs[i], slots, r["T_slots"], cam, p)
+        assert np.array_equal(dm.getDebugmap(), o["sparse"]), i
+    assert n_dense >= 3
