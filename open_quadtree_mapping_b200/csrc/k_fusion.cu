@@ -133,10 +133,15 @@ __global__ void __launch_bounds__(kFlatThreads)
     mu = dep;
     s2 = 2500.0;
   }
-  // The reference's formulas with each shared denominator inverted once (FP64
-  // division is the costly operation here); the results differ from the
-  // term-by-term quotients by a few FP64 ulps.  The inlier ratio that gates
-  // the output is the exact quotient.
+  // The reference's formulas with their denominators shared and inverted once
+  // (FP64 division is the costly operation here: five of them instead of
+  // the reference's term-by-term quotients; the results differ from those
+  // by a few FP64 ulps).  The identities used: c1 = ratio * pdf and
+  // c2 = b / (a + b) / 50 are both rescaled by (a + b) before the
+  // normalisation, which cancels it; 1/(ab+1) and 1/(ab+2) come from
+  // 1/((ab+1)(ab+2)); and a' = (e - f) / (f - e/f), b' = a' (1 - f) / f
+  // share the denominator f^2 - e.  The inlier ratio that gates the output
+  // is the exact quotient.
   const double var = unc + s2;
   const double ivar = 1.0 / var;
   const double new_sq = unc * s2 * ivar;
@@ -145,19 +150,20 @@ __global__ void __launch_bounds__(kFlatThreads)
   const double pdf = exp(-dm * dm * (0.5 * ivar)) * rsqrt(2.0 * M_PI * var);
   const double ab = a + b;
   const double ratio = a / ab;
-  double c1 = ratio * pdf;
-  double c2 = b * (1.0 / ab) * (1.0 / 50.0);
+  double c1 = a * pdf;
+  double c2 = b * (1.0 / 50.0);
   const double inorm = 1.0 / (c1 + c2);
   c1 *= inorm;
   c2 *= inorm;
-  const double i1 = 1.0 / (ab + 1.0), i2 = 1.0 / (ab + 2.0);
+  const double i12 = 1.0 / ((ab + 1.0) * (ab + 2.0));
+  const double i1 = (ab + 2.0) * i12;
   const double f = (c1 * (a + 1.0) + c2 * a) * i1;
-  const double e = (c1 * ((a + 1.0) * (a + 2.0)) + c2 * (a * (a + 1.0))) * (i1 * i2);
+  const double e = (c1 * ((a + 1.0) * (a + 2.0)) + c2 * (a * (a + 1.0))) * i12;
   const double mu_p = c1 * new_mu + c2 * mu;
   const double s2_p = c1 * (new_sq + new_mu * new_mu) + c2 * (s2 + mu * mu) - mu_p * mu_p;
-  const double inv_f = 1.0 / f;
-  const double a_p = (e - f) / (f - e * inv_f);
-  const double b_p = a_p * (1.0 - f) * inv_f;
+  const double q = (e - f) / (f * f - e);
+  const double a_p = q * f;
+  const double b_p = q * (1.0 - f);
   J.dense[idx] = (ratio > 0.60) ? (float)mu_p : -1.0f;
   J.seeds_out[idx] = make_float4((float)a_p, (float)b_p, (float)mu_p, (float)s2_p);
 }
