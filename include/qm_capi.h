@@ -231,7 +231,11 @@ int qm_batch_stream(qm_batch *b, void **stream);
 /* Kernel kinds reported by qm_batch_profile, in this order. */
 #define QM_NUM_KERNEL_KINDS 11
 /* quadtree, cost, pyramid, message init/upsample, bp half-sweep, extraction,
- * row solve, column solve, fuse transform, hole fill, fuse update.  Runs the resident pipeline once with eager launches, each
+ * row solve, column solve, fuse transform, hole fill, fuse update.  The
+ * message-init kind launches only at levels with fewer than two half-sweeps
+ * (otherwise the half-sweeps write the inherited messages), and the hole-fill
+ * kind reports 0 launches: hole filling runs inside the fuse update.  Runs
+ * the resident pipeline once with eager launches, each
  * bracketed by CUDA events; ms[k] and launches[k] receive the summed device
  * time and the launch count of kind k.  No counterpart in the reference
  * (its printf timers measure CPU clock time, seed_matrix.cu:482-546). */

@@ -35,13 +35,14 @@ enum KernelKind
   kQuadtree = 0,
   kCost,
   kPyramid,
-  kMsgInit,
+  kMsgInit, // levels with fewer than two half-sweeps only
   kSweep,
   kExtract,
   kRowSolve,
   kColSolve,
   kFuseTransform,
-  kFuseFill,
+  kFuseFill, // not launched (hole filling runs inside kFuseUpdate); keeps the
+             // kind indices of qm_batch_profile stable
   kFuseUpdate,
   kNumKinds
 };
