@@ -3,9 +3,11 @@
 // Stage order of one run, after SeedMatrix::extract_depth and
 // fuse_output_depth (seed_matrix.cu:448-597):
 //   quadtree -> cost -> pyramid(1..L-1) ->
-//   for level L-1..0: message inheritance + bp half-sweeps
-//     (+ extraction at level 0) ->
-//   row solve -> column solve -> fuse transform -> hole fill -> fuse update.
+//   for level L-1..0: bp half-sweeps (the first two also write the
+//     inherited messages; a separate inheritance pass only at levels with
+//     fewer than two) (+ extraction at level 0) ->
+//   row solve (also resets the fusion keys) -> column solve ->
+//   fuse transform -> fuse update (hole filling inside).
 // Every stage is one launch over all active jobs (one per hypothesis count
 // for the warp-per-cell BP kernels); optionally the BP stages of a level run
 // over consecutive job ranges whose level working set fits a byte budget, so
