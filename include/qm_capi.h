@@ -87,9 +87,14 @@ int qm_version(void); /* major*10000 + minor*100 + patch */
  * quadmap::Depthmap (depthmap.h:34-75, depthmap.cpp:19-68).  One camera
  * stream: frame ring, frame-selection policy of SeedMatrix::add_frames
  * (seed_matrix.cu:106-209), dense extraction and fusion.  The semi-dense
- * tracker is not part of this library, so its projected depths are absent
- * from the sparse input of the upsampler (the debug map holds the BP node
- * depths only).  The image is expected undistorted (the reference's host
+ * tracker (seed_matrix.cu:120-140) is built but off by default: until
+ * qm_depthmap_set_semidense(h, 1) the upsampler's sparse input and the debug
+ * map hold the BP node depths only; with it on, the tracker's projected
+ * depths join them as in the reference.  With the tracker on, results agree
+ * with the reference's own tracker kernels but are not identical to them:
+ * the reference resolves pixel collisions and in-place neighbourhood passes
+ * by thread scheduling, this library by fixed rules (nearest wins, Jacobi
+ * passes).  The image is expected undistorted (the reference's host
  * cv::remap, seed_matrix.cu:85, stays with the caller). */
 typedef struct qm_depthmap qm_depthmap;
 
@@ -297,7 +302,9 @@ int qm_upsample(const float *sparse, const uint8_t *img, size_t img_pitch, int w
  * allocates nothing: the row-pass scratch is a fixed device array of this
  * library of QM_UPSAMPLE_NOALLOC_MAX_PIXELS pixels (8 bytes each); larger
  * images return QM_ERR_INVALID_ARG.  The first call on a device sets up that
- * device (make it before any stream capture).  All calls on a device share
+ * device (make it before any stream capture); so does the first call under
+ * a different CUDA context (after cudaDeviceReset, or a context the host
+ * made current itself), since the array's address is per context.  All calls on a device share
  * the scratch: calls that can overlap on the device race and give undefined
  * output, so issue them in order (e.g. on one stream).  Same limits as
  * qm_upsample otherwise. */

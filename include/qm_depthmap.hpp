@@ -6,8 +6,12 @@
 // overloads are compiled when QM_WITH_OPENCV is defined (the ROS node's
 // build); raw-buffer overloads are always available.  Poses accept the
 // reference's SE3<float> (anything with data[0..11] in row-major 3x4 order)
-// or a float[12].  Errors from the library are thrown as quadmap::QmError
-// (the reference throws quadmap::CudaException, cuda_exception.cuh:26-44).
+// or a float[12]; getT_world_ref() returns a QmPose, which converts
+// implicitly to the reference's SE3<float>, so the publisher's
+// `const quadmap::SE3<float> T_world_ref = depthmap_->getT_world_ref();`
+// (publisher.cpp:138) compiles unchanged.  Errors from the library are
+// thrown as quadmap::QmError (the reference throws quadmap::CudaException,
+// cuda_exception.cuh:26-44).
 #pragma once
 
 #include <cstddef>
@@ -15,6 +19,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "qm_capi.h"
@@ -37,6 +42,24 @@ inline void qm_check(int status)
   if (status != QM_OK)
     throw QmError(status, std::string("libqm_b200: ") + qm_last_error());
 }
+
+// A rigid transform as 12 floats, row-major 3x4 [R | t] (the layout of the
+// reference's SE3<float>::data, se3.cuh).  Converts implicitly to any pose
+// type whose `data` member takes data[0..11] = float, the reference's
+// quadmap::SE3<float> among them.
+struct QmPose
+{
+  float data[12];
+
+  template <class SE3T, class = decltype(std::declval<SE3T &>().data[0] = 0.0f)>
+  operator SE3T() const
+  {
+    SE3T s;
+    for (int i = 0; i < 12; ++i)
+      s.data[i] = data[i];
+    return s;
+  }
+};
 
 class Depthmap
 {
@@ -73,12 +96,16 @@ public:
     const bool has = add_frames(und.data, und.step, T);
     if (has)
     {
-      depth_out_.create((int)height_, (int)width_);
-      debug_out_.create((int)height_, (int)width_);
-      reference_out_.create((int)height_, (int)width_, CV_8UC1);
-      getDepthmap((float *)depth_out_.data, depth_out_.step / sizeof(float));
-      getDebugmap((float *)debug_out_.data, debug_out_.step / sizeof(float));
-      getReferenceImage(reference_out_.data, reference_out_.step);
+      // fresh buffers per result, as SeedMatrix::get_result clones
+      // (seed_matrix.cu:607-612): maps a caller still holds stay unchanged
+      cv::Mat_<float> depth((int)height_, (int)width_), debug((int)height_, (int)width_);
+      cv::Mat reference((int)height_, (int)width_, CV_8UC1);
+      getDepthmap((float *)depth.data, depth.step / sizeof(float));
+      getDebugmap((float *)debug.data, debug.step / sizeof(float));
+      getReferenceImage(reference.data, reference.step);
+      depth_out_ = depth;
+      debug_out_ = debug;
+      reference_out_ = reference;
     }
     return has;
   }
@@ -133,6 +160,15 @@ public:
   {
     for (int i = 0; i < 12; ++i)
       T[i] = T_world_ref_[i];
+  }
+  // getT_world_ref (depthmap.h:74): world <- reference frame of the last
+  // result; assign it to the reference's SE3<float> directly.
+  QmPose getT_world_ref() const
+  {
+    QmPose p;
+    for (int i = 0; i < 12; ++i)
+      p.data[i] = T_world_ref_[i];
+    return p;
   }
   template <class SE3T>
   SE3T getT_world_ref() const

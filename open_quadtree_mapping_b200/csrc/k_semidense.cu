@@ -277,9 +277,19 @@ __global__ void __launch_bounds__(kSdThreads) k_sd_init(const __grid_constant__ 
   store_seed(J, 0, o, s);
 }
 
+// Sum of the products of two five-sample residual sets, left to right.
+template <bool I>
+__device__ __forceinline__ Fl<I> residual_overlap(const Fl<I> (&a)[5], const Fl<I> (&b)[5])
+{
+  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2] + a[3] * b[3] + a[4] * b[4];
+}
+
 // search_point (lsd_semidense.cu:517-754): epipolar line search of the
 // keyframe pixel (x, y) in the incoming image.  Returns the match error or a
-// negative failure code.
+// negative failure code.  The operation order follows the reference's so
+// that reference arithmetic rounds as it does; the residuals of the last even
+// and the last odd step are kept apart because the sub-pixel step uses their
+// overlap on both sides of the best match.
 template <bool I>
 __device__ float search_point(const SdJob &J, int x, int y, float2 epi, Fl<I> gradient_max,
                               Fl<I> my_gradient, Fl<I> min_idep, Fl<I> max_idep,
@@ -288,27 +298,30 @@ __device__ float search_point(const SdJob &J, int x, int y, float2 epi, Fl<I> gr
   using F = Fl<I>;
   const F fx(J.fx), fy(J.fy), cx(J.cx), cy(J.cy);
   const float *T = J.T;
-  F this_patch[5];
+  // five keyframe samples along the epipolar direction, centred on (x, y)
+  F key_patch[5];
 #pragma unroll
   for (int i = -2; i <= 2; i++)
   {
     const F px = F((float)x) + F((float)i) * F(epi.x);
     const F py = F((float)y) + F((float)i) * F(epi.y);
-    this_patch[i + 2] = sample<I>(J.key_tex, J.key_f, J.pitch, J.W, J.H, plus_d(px.v, 0.5),
-                                  plus_d(py.v, 0.5));
+    key_patch[i + 2] = sample<I>(J.key_tex, J.key_f, J.pitch, J.W, J.H, plus_d(px.v, 0.5),
+                                 plus_d(py.v, 0.5));
   }
-  // far and near points of the search range
+  // the pixel's ray rotated into the incoming camera and projected (K R K^-1
+  // p, homogeneous), and the projected translation (K t): a point at
+  // inverse depth q lands at ray + q * shift
   const F kx = (F((float)x) - cx) / fx, ky = (F((float)y) - cy) / fy, kz(1.0f);
   const F rx = F(T[0]) * kx + F(T[1]) * ky + F(T[2]) * kz;
   const F ry = F(T[4]) * kx + F(T[5]) * ky + F(T[6]) * kz;
   const F rz = F(T[8]) * kx + F(T[9]) * ky + F(T[10]) * kz;
   const F tx(T[3]), ty(T[7]), tz(T[11]);
-  const F KRKiPx = fx * rx + cx * rz, KRKiPy = fy * ry + cy * rz, KRKiPz = rz;
-  const F KTx = fx * tx + cx * tz, KTy = fy * ty + cy * tz, KTz = tz;
-  const F nearx = KRKiPx + KTx * max_idep, neary = KRKiPy + KTy * max_idep,
-          nearz = KRKiPz + KTz * max_idep;
-  const F farx = KRKiPx + KTx * min_idep, fary = KRKiPy + KTy * min_idep,
-          farz = KRKiPz + KTz * min_idep;
+  const F ray_x = fx * rx + cx * rz, ray_y = fy * ry + cy * rz, ray_z = rz;
+  const F shift_x = fx * tx + cx * tz, shift_y = fy * ty + cy * tz, shift_z = tz;
+  const F nearx = ray_x + shift_x * max_idep, neary = ray_y + shift_y * max_idep,
+          nearz = ray_z + shift_z * max_idep;
+  const F farx = ray_x + shift_x * min_idep, fary = ray_y + shift_y * min_idep,
+          farz = ray_z + shift_z * min_idep;
   F near_u = nearx / nearz, near_v = neary / nearz;
   F far_u = farx / farz, far_v = fary / farz;
   const F du = near_u - far_u, dv = near_v - far_v;
@@ -326,21 +339,24 @@ __device__ float search_point(const SdJob &J, int x, int y, float2 epi, Fl<I> gr
       far_v.v >= (float)(J.H - 2))
     return -1.0f;
 
-  F that_patch[5];
+  // five incoming-image samples ending at the current step, oldest first
+  F line_patch[5];
 #pragma unroll
   for (int i = -2; i <= 1; i++)
   {
     const F px = far_u + F((float)i) * dir_u, py = far_v + F((float)i) * dir_v;
-    that_patch[i + 2] = sample<I>(J.inc_tex, J.inc_f, J.pitch, J.W, J.H, plus_d(px.v, 0.5),
+    line_patch[i + 2] = sample<I>(J.inc_tex, J.inc_f, J.pitch, J.W, J.H, plus_d(px.v, 0.5),
                                   plus_d(py.v, 0.5));
   }
-  F best_step(-1.0f), best_score(1e9f), pre_best_score(1e9f), post_best_score(1e9f);
+  F best_step(-1.0f), best_score(1e9f), score_before_best(1e9f), score_after_best(1e9f);
   bool last_is_best = false;
-  F best_pre(NAN), best_post(NAN);
-  F e1A(NAN), e1B(NAN), e2A(NAN), e2B(NAN), e3A(NAN), e3B(NAN), e4A(NAN), e4B(NAN), e5A(NAN),
-      e5B(NAN);
+  F overlap_before(NAN), overlap_after(NAN);
+  F res_even[5], res_odd[5];
+#pragma unroll
+  for (int j = 0; j < 5; ++j)
+    res_even[j] = res_odd[j] = F(NAN);
   F second_best_score(1e9f), second_best_step(-1.0f);
-  F pre_score(1e9f), this_score(1e9f);
+  F prev_score(1e9f), score(1e9f);
   // the sample of step s + 1 is fetched while step s is scored (sampling is
   // a pure function of its coordinates and clamps, so the fetch past the last
   // step is harmless)
@@ -353,66 +369,58 @@ __device__ float search_point(const SdJob &J, int x, int y, float2 epi, Fl<I> gr
   F next = fetch(0);
   for (int step = 0; (float)step <= search_length.v && step <= kMaxSearch; step += 1)
   {
-    pre_score = this_score;
-    this_score = F(0.0f);
+    prev_score = score;
+    score = F(0.0f);
     const F sx = far_u + F((float)step) * dir_u, sy = far_v + F((float)step) * dir_v;
     if (sx.v <= 1.0f || sx.v >= (float)(J.W - 1) || sy.v <= 1.0f || sy.v >= (float)(J.H - 1))
       break;
-    that_patch[4] = next;
+    line_patch[4] = next;
     next = fetch(step + 1);
+    // squared residuals, newest sample first
     if (step % 2 == 0)
     {
-      e1A = that_patch[4] - this_patch[4];
-      this_score = this_score + e1A * e1A;
-      e2A = that_patch[3] - this_patch[3];
-      this_score = this_score + e2A * e2A;
-      e3A = that_patch[2] - this_patch[2];
-      this_score = this_score + e3A * e3A;
-      e4A = that_patch[1] - this_patch[1];
-      this_score = this_score + e4A * e4A;
-      e5A = that_patch[0] - this_patch[0];
-      this_score = this_score + e5A * e5A;
+#pragma unroll
+      for (int j = 0; j < 5; ++j)
+      {
+        res_even[j] = line_patch[4 - j] - key_patch[4 - j];
+        score = score + res_even[j] * res_even[j];
+      }
     }
     else
     {
-      e1B = that_patch[4] - this_patch[4];
-      this_score = this_score + e1B * e1B;
-      e2B = that_patch[3] - this_patch[3];
-      this_score = this_score + e2B * e2B;
-      e3B = that_patch[2] - this_patch[2];
-      this_score = this_score + e3B * e3B;
-      e4B = that_patch[1] - this_patch[1];
-      this_score = this_score + e4B * e4B;
-      e5B = that_patch[0] - this_patch[0];
-      this_score = this_score + e5B * e5B;
+#pragma unroll
+      for (int j = 0; j < 5; ++j)
+      {
+        res_odd[j] = line_patch[4 - j] - key_patch[4 - j];
+        score = score + res_odd[j] * res_odd[j];
+      }
     }
     if (last_is_best)
     {
-      post_best_score = this_score;
-      best_post = e1A * e1B + e2A * e2B + e3A * e3B + e4A * e4B + e5A * e5B;
+      score_after_best = score;
+      overlap_after = residual_overlap<I>(res_even, res_odd);
       last_is_best = false;
     }
-    if (this_score < best_score)
+    if (score < best_score)
     {
       second_best_score = best_score;
       second_best_step = best_step;
-      best_score = this_score;
+      best_score = score;
       best_step = F((float)step);
-      pre_best_score = pre_score;
-      best_pre = e1A * e1B + e2A * e2B + e3A * e3B + e4A * e4B + e5A * e5B;
-      best_post = F(-1.0f);
-      post_best_score = F(1e9f);
+      score_before_best = prev_score;
+      overlap_before = residual_overlap<I>(res_even, res_odd);
+      overlap_after = F(-1.0f);
+      score_after_best = F(1e9f);
       last_is_best = true;
     }
-    else if (this_score < second_best_score)
+    else if (score < second_best_score)
     {
-      second_best_score = this_score;
+      second_best_score = score;
       second_best_step = F((float)step);
     }
-    that_patch[0] = that_patch[1];
-    that_patch[1] = that_patch[2];
-    that_patch[2] = that_patch[3];
-    that_patch[3] = that_patch[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      line_patch[j] = line_patch[j + 1];
   }
 
   if (best_score > F(4.0f * kMaxErrorStereo))
@@ -421,33 +429,37 @@ __device__ float search_point(const SdJob &J, int x, int y, float2 epi, Fl<I> gr
       F(kMinDistErrorStereo) * best_score > second_best_score)
     return -2.0f;
 
+  // sub-pixel refinement from the score slopes on either side of the best
+  // step
   F best_match_sub = best_step;
   bool did_subpixel = false;
   {
-    const F grad_pre_pre = -(pre_best_score - best_pre);
-    const F grad_pre_this = best_score - best_pre;
-    const F grad_post_this = -(best_score - best_post);
-    const F grad_post_post = post_best_score - best_post;
-    bool interp_post = false, interp_pre = false;
-    if ((grad_pre_pre.v < 0.0f) ^ (grad_pre_this.v < 0.0f))
+    const F slope_before_out = -(score_before_best - overlap_before);
+    const F slope_before_in = best_score - overlap_before;
+    const F slope_after_in = -(best_score - overlap_after);
+    const F slope_after_out = score_after_best - overlap_after;
+    bool use_after = false, use_before = false;
+    if ((slope_before_out.v < 0.0f) ^ (slope_before_in.v < 0.0f))
     {
-      if (!((grad_post_post.v < 0.0f) ^ (grad_post_this.v < 0.0f)))
-        interp_pre = true;
+      if (!((slope_after_out.v < 0.0f) ^ (slope_after_in.v < 0.0f)))
+        use_before = true;
     }
-    else if ((grad_post_post.v < 0.0f) ^ (grad_post_this.v < 0.0f))
-      interp_post = true;
-    if (interp_pre)
+    else if ((slope_after_out.v < 0.0f) ^ (slope_after_in.v < 0.0f))
+      use_after = true;
+    if (use_before)
     {
-      const F d = grad_pre_this / (grad_pre_this - grad_pre_pre);
+      const F d = slope_before_in / (slope_before_in - slope_before_out);
       best_match_sub = best_match_sub - d;
-      best_score = best_score - F(2.0f) * d * grad_pre_this - (grad_pre_pre - grad_pre_this) * d * d;
+      best_score = best_score - F(2.0f) * d * slope_before_in -
+                   (slope_before_out - slope_before_in) * d * d;
       did_subpixel = true;
     }
-    else if (interp_post)
+    else if (use_after)
     {
-      const F d = grad_post_this / (grad_post_this - grad_post_post);
+      const F d = slope_after_in / (slope_after_in - slope_after_out);
       best_match_sub = best_match_sub - d;
-      best_score = best_score + F(2.0f) * d * grad_post_this + (grad_post_post - grad_post_this) * d * d;
+      best_score = best_score + F(2.0f) * d * slope_after_in +
+                   (slope_after_out - slope_after_in) * d * d;
       did_subpixel = true;
     }
   }
@@ -456,22 +468,26 @@ __device__ float search_point(const SdJob &J, int x, int y, float2 epi, Fl<I> gr
 #pragma unroll
   for (int i = 1; i < 5; i++)
     grad_along_line =
-        grad_along_line + (this_patch[i] - this_patch[i - 1]) * (this_patch[i] - this_patch[i - 1]);
+        grad_along_line + (key_patch[i] - key_patch[i - 1]) * (key_patch[i] - key_patch[i - 1]);
   if (best_score > F(kMaxErrorStereo) + fsqrt(grad_along_line) * F(20.0f))
     return -3.0f;
 
+  // inverse depth of the match from the coordinate that moves most along the
+  // line, and its derivative with respect to that coordinate
   F best_idepth, alpha;
   if (dir_u * dir_u > dir_v * dir_v)
   {
     const F best_u = far_u + best_match_sub * dir_u;
-    best_idepth = (best_u * KRKiPz - KRKiPx) / (KTx - best_u * KTz);
-    alpha = (KRKiPz * KTx - KTz * KRKiPx) / ((KTx - best_u * KTz) * (KTx - best_u * KTz));
+    best_idepth = (best_u * ray_z - ray_x) / (shift_x - best_u * shift_z);
+    alpha = (ray_z * shift_x - shift_z * ray_x) /
+            ((shift_x - best_u * shift_z) * (shift_x - best_u * shift_z));
   }
   else
   {
     const F best_v = far_v + best_match_sub * dir_v;
-    best_idepth = (best_v * KRKiPz - KRKiPy) / (KTy - best_v * KTz);
-    alpha = (KRKiPz * KTy - KTz * KRKiPy) / ((KTy - best_v * KTz) * (KTy - best_v * KTz));
+    best_idepth = (best_v * ray_z - ray_y) / (shift_y - best_v * shift_z);
+    alpha = (ray_z * shift_y - shift_z * ray_y) /
+            ((shift_y - best_v * shift_z) * (shift_y - best_v * shift_z));
   }
   best_idepth = (double)best_idepth.v < 0.01 ? F(kMinInvDepth) : best_idepth;
   best_idepth = (double)best_idepth.v > 2.0 ? F(kMaxInvDepth) : best_idepth;

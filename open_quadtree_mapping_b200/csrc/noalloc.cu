@@ -16,12 +16,16 @@
 // Set-up: the first call on a device (with that device current) looks up the
 // array's device address with cudaGetSymbolAddress, which may load this
 // library's device code on that device; make that first call before any
-// stream capture begins.  Later calls on the same device reuse the address.
+// stream capture begins.  Later calls reuse the address while the same CUDA
+// context is current; a call under another context (after cudaDeviceReset,
+// or with a context the host created and made current itself) looks it up
+// again, because the module, and so the array, may sit elsewhere there.
 //
 // All calls on one device share the one array: two calls whose work can
 // overlap on the device (different streams, or different host threads
 // without ordering) race on it and both outputs are undefined.  Serialise
 // them, e.g. issue them on one stream.
+#include <cuda.h>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -40,10 +44,53 @@ __device__ __align__(256) float2 g_upsample_scratch[kScratchPixels];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
-float2 *g_scratch_of_device[kMaxDevices] = {};
+
+// The scratch address of each device, with the id of the context it was
+// looked up under (0: none yet).
+struct ScratchAddr
+{
+  unsigned long long ctx_id;
+  float2 *ptr;
+};
+ScratchAddr g_scratch_of_device[kMaxDevices] = {};
+
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long *);
+
+// Unique id of the context current on this thread, 0 when none is current
+// or the driver cannot say (then the address is looked up on every call).
+unsigned long long current_context_id()
+{
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static bool resolved = false;
+  if (!resolved)
+  {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(f);
+    cudaGetLastError();
+    resolved = true;
+  }
+  if (!get_current || !get_id)
+    return 0;
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&ctx) != CUDA_SUCCESS || ctx == nullptr || get_id(ctx, &id) != CUDA_SUCCESS)
+    return 0;
+  return id;
+}
 
 // Device address of the scratch array on the current device, looked up once
-// per device.
+// per device and context.
 float2 *scratch_for_current_device()
 {
   int dev = -1;
@@ -51,19 +98,22 @@ float2 *scratch_for_current_device()
   if (dev < 0 || dev >= kMaxDevices)
     throw CudaError{QM_ERR_INVALID_ARG, "qm_upsample_noalloc: device ordinal out of range"};
   std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (g_scratch_of_device[dev] == nullptr)
+  ScratchAddr &slot = g_scratch_of_device[dev];
+  const unsigned long long ctx = current_context_id();
+  if (ctx != 0 && slot.ctx_id == ctx && slot.ptr != nullptr)
+    return slot.ptr;
+  void *p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_upsample_scratch);
+  if (e != cudaSuccess || p == nullptr)
   {
-    void *p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_upsample_scratch);
-    if (e != cudaSuccess || p == nullptr)
-    {
-      cudaGetLastError();
-      throw CudaError{QM_ERR_CUDA, std::string("qm_upsample_noalloc: cudaGetSymbolAddress: ") +
-                                       cudaGetErrorString(e)};
-    }
-    g_scratch_of_device[dev] = static_cast<float2 *>(p);
+    cudaGetLastError();
+    throw CudaError{QM_ERR_CUDA, std::string("qm_upsample_noalloc: cudaGetSymbolAddress: ") +
+                                     cudaGetErrorString(e)};
   }
-  return g_scratch_of_device[dev];
+  // the lookup may have made the device's primary context current
+  slot.ctx_id = ctx != 0 ? ctx : current_context_id();
+  slot.ptr = static_cast<float2 *>(p);
+  return slot.ptr;
 }
 
 void fail_if(bool bad, const char *msg)

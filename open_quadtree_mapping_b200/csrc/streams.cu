@@ -431,6 +431,19 @@ void StreamSet::step(const std::vector<int> &which, const uint8_t *const *imgs,
                      const size_t *strides, const float *T_curr_world, int *has_result,
                      float *const *depth_outs, const size_t *depth_strides)
 {
+  // every argument is checked before any stream's state changes, so a
+  // rejected call leaves the set as it was and launches nothing: the cost
+  // kernel gathers measurement pixels without clamping and relies on poses
+  // that keep projections finite
+  for (size_t k = 0; k < which.size(); ++k)
+  {
+    const int i = which[k];
+    if (!imgs[k] || strides[k] < (size_t)st_[i].d.W)
+      throw CudaError{QM_ERR_INVALID_ARG, "image pointer or stride invalid"};
+    if (!rigid_enough(T_curr_world + 12 * k))
+      throw CudaError{QM_ERR_INVALID_ARG,
+                      "frame pose is not a rigid transform (finite, rotation rows bounded)"};
+  }
   check(cudaSetDevice(device_), "cudaSetDevice");
   const int p = (int)(step_ & 1);
   // step t-2 (same parity) must be done: its output buffer, pinned tables

@@ -7,7 +7,11 @@
 // src/lsd_semidense.cu, are #included by path; see oracle/Makefile), with the
 // reference's flags (-O3 -use_fast_math) for sm_100a.  Only the legacy texture
 // references are swapped for texture objects (ref_shim/quadmap/
-// texture_memory.cuh) and <opencv2/opencv.hpp> for an empty header.
+// texture_memory.cuh) and <opencv2/opencv.hpp> for an empty header.  The
+// same file also builds the patched variants (other DEPTH_NUM and inverse-
+// depth range, oracle/refpatch.py): every per-hypothesis launch below takes
+// DEPTH_NUM threads where the reference's host code writes 64, which is the
+// reference's own launch when DEPTH_NUM is 64.
 //
 // The extern "C" functions below replay the host sequences of
 // SeedMatrix::extract_depth (src/seed_matrix.cu:448-551) and
@@ -81,11 +85,13 @@ void bp_keep_messages(DeviceImage<PIXEL_COST> &image_cost_map, float *msg_out)
   pyr[0] = &image_cost_map;
   for (int i = 1; i < hbp_level; i++)
     pyr[i] = new DeviceImage<PIXEL_COST>(h_width[i], h_height[i]);
+  // bpextract.cu:67-78; with more than 64 hypotheses (a patched build)
+  // the z extent is split over DEPTH_NUM / 64 blocks
   dim3 hb;
   hb.z = 64;
   for (int i = 1; i < hbp_level; i++)
   {
-    dim3 hg(h_width[i], h_height[i]);
+    dim3 hg(h_width[i], h_height[i], DEPTH_NUM / 64);
     cost_distribute<<<hg, hb>>>(pyr[i - 1]->dev_ptr, pyr[i]->dev_ptr);
     cudaDeviceSynchronize();
   }
@@ -102,7 +108,7 @@ void bp_keep_messages(DeviceImage<PIXEL_COST> &image_cost_map, float *msg_out)
       DeviceImage<PIXEL_COST> *next[4];
       for (int m = 0; m < 4; ++m)
         next[m] = new DeviceImage<PIXEL_COST>(h_width[lv], h_height[lv]);
-      dim3 ub(64);
+      dim3 ub(DEPTH_NUM);
       dim3 ug(h_width[lv + 1], h_height[lv + 1]);
       for (int m = 0; m < 4; m++)
         upsample<<<ug, ub>>>(msg[m]->dev_ptr, next[m]->dev_ptr);
@@ -113,7 +119,7 @@ void bp_keep_messages(DeviceImage<PIXEL_COST> &image_cost_map, float *msg_out)
         msg[m] = next[m];
       }
     }
-    dim3 bb(4, 64);
+    dim3 bb(4, DEPTH_NUM);
     dim3 bg((h_width[lv] + 1) / 2, h_height[lv]);
     bool A_set = true;
     for (int it = 0; it < hbp_iterate[lv]; it++)
@@ -185,10 +191,10 @@ void run_extract(ExtractState &st, int nslots, DeviceImage<float> &debug_image,
   DeviceImage<int> add_num(st.w / 4, st.h / 4);
   image_cost.zero();
   add_num.zero();
-  dim3 cb(64, nslots);
+  dim3 cb(DEPTH_NUM, nslots);
   dim3 cg(st.w / 4, st.h / 4);
   image_to_cost<<<cg, cb>>>(st.mp.dev_ptr, st.age.dev_ptr, image_cost.dev_ptr, add_num.dev_ptr);
-  dim3 nb(64);
+  dim3 nb(DEPTH_NUM);
   normalize_the_cost<<<cg, nb>>>(image_cost.dev_ptr, add_num.dev_ptr);
   cudaDeviceSynchronize();
 
@@ -245,20 +251,28 @@ int status()
 
 extern "C" {
 
+// The constants this build was compiled with: the reference's own
+// (64, 0.01, (2.0 - 0.01) / 63) or a patched variant's (oracle/refpatch.py).
+int qmref_depth_num() { return DEPTH_NUM; }
+double qmref_min_inv_depth() { return MIN_INV_DEPTH; }
+double qmref_inv_depth_step() { return STEP_INV_DEPTH; }
+
 // Depth extraction as SeedMatrix::extract_depth does it.
 //   income_img  w*h float (values 0..255)
 //   frames_img  nframes*w*h float, ring order (index 0 = most recent)
 //   T_frame_income  nframes*12 floats, row-major 3x4 T_frame<-income
-//   nslots      measurement slots (blockDim.y of image_to_cost; reference 5)
+//   nslots      measurement slots (blockDim.y of image_to_cost; reference 5;
+//               DEPTH_NUM * nslots threads must fit one block, <= 1024)
 //   debug_inout w*h: sparse prior in, sparse BP depth out
-// Optional outputs (NULL to skip): levels (w*h int), cost ((w/4)*(h/4)*64),
-// msg (4 x (w/4)*(h/4)*64, order up, down, left, right), dense (w*h).
+// Optional outputs (NULL to skip): levels (w*h int), cost ((w/4)*(h/4)*DEPTH_NUM),
+// msg (4 x (w/4)*(h/4)*DEPTH_NUM, order up, down, left, right), dense (w*h).
 int qmref_extract(int w, int h, float fx, float fy, float cx, float cy, const float *income_img,
                   int nframes, const float *frames_img, const float *T_frame_income, int nslots,
                   float *debug_inout, int *levels_out, float *cost_out, float *msg_out,
                   float *dense_out)
 {
-  if (nframes < 1 || nframes > KEYFRAME_NUM || nslots < 1 || nslots > 10)
+  if (nframes < 1 || nframes > KEYFRAME_NUM || nslots < 1 || nslots > 10 ||
+      DEPTH_NUM * nslots > 1024)
     return 1;
   try
   {
@@ -324,7 +338,8 @@ int qmref_time_frames(int w, int h, float fx, float fy, float cx, float cy,
                       const float *T_frame_income, int nslots, const float *T_income_last,
                       int warmup, int iters, double *ms_per_frame)
 {
-  if (nframes < 1 || nframes > KEYFRAME_NUM || nslots < 1 || nslots > 10 || iters < 1)
+  if (nframes < 1 || nframes > KEYFRAME_NUM || nslots < 1 || nslots > 10 ||
+      DEPTH_NUM * nslots > 1024 || iters < 1)
     return 1;
   try
   {

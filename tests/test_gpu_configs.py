@@ -5,6 +5,11 @@
   volume, labels and sparse depths bit-exact with the oracle; upsampled depth
   within 1e-5 relative of the FP64 oracle for 99.9 % of the pixels and
   1e-4 for all.
+* Video sequence: one stream at 1280x720 (fx = fy = 780), 64 hypotheses,
+  10 measurement slots, 30 frames with Bayesian fusion across keyframes,
+  IEEE arithmetic, against an oracle replay of the same frame policy: debug
+  map (sparse BP depths) bit-exact on every dense frame; fused depth and
+  variance within 1e-5 relative at the 99th percentile.
 * Uneven batch: 16 streams (6 at 640x480, 6 at 752x480, 4 at 1280x720), 3-10
   measurement frames and 48/64/96 hypotheses per stream, one launch per
   stage: every stream's fused depth bit-identical to the same stream run
@@ -24,6 +29,7 @@ from open_quadtree_mapping_b200.params import ARITH_IEEE, Params
 pytestmark = pytest.mark.gpu
 
 UPSAMPLE_RTOL = 1e-5
+FUSE_RTOL = 1e-5
 
 
 def _render(args):
@@ -71,6 +77,64 @@ def test_large_keyframe_vs_oracle(oracle_mod, gpu):
     rel = np.abs(g["dense"][ok] - d64[ok]) / d64[ok]
     stats = (np.percentile(rel, 99.9), rel.max())
     assert stats[0] < UPSAMPLE_RTOL and stats[1] < 10 * UPSAMPLE_RTOL, stats
+
+
+def test_video_720p_sequence_vs_oracle_replay(oracle_mod, gpu):
+    """The 720p, 10-slot, 30-frame sequence through the batched engine (one
+    stream; the facade is fixed at the reference's 5 slots) against the
+    oracle replaying the same frame policy: quadtree, cost, BP and
+    extraction in IEEE arithmetic equal the oracle bit for bit, so the debug
+    map must too; the upsampled depth (FP32 right-hand sides here, FP64 in
+    the replay) and the FP64 fusion then agree within FUSE_RTOL."""
+    from open_quadtree_mapping_b200 import synthetic as syn
+    from open_quadtree_mapping_b200.depthmap import BatchDepthmap
+    from oracle.policy import PolicyReplay
+    W, H, f, F, n, s = 1280, 720, 780.0, 10, 30, 41
+    traj = syn.make_trajectory(2000 + s, n)
+    imgs = _render_all([(1000 + s, traj[i], W, H, f) for i in range(n)])
+    imgs = [im for im, _ in imgs]
+    Ts = [np.ascontiguousarray(syn.inv_se3(traj[i])[:3, :4].reshape(-1), np.float32)
+          for i in range(n)]
+    cam = (f, f, W / 2.0, H / 2.0)
+    p = Params(arith=ARITH_IEEE)
+    b = BatchDepthmap([dict(width=W, height=H, fx=f, fy=f, cx=W / 2.0, cy=H / 2.0, num_hyp=64,
+                            num_slots=F)], params=p)
+    pol = PolicyReplay(num_slots=F)
+    oracle_mod.set_threads(8)
+    seeds = np.zeros((H, W, 4), np.float32)
+    n_dense = n_valid = n_oracle_valid = 0
+    worst_depth = worst_var = 0.0
+    for i in range(n):
+        has = b.add_frames([imgs[i]], [Ts[i]])[0]
+        r = pol.add(i, Ts[i])
+        assert has == (r["outcome"] in ("first", "dense")), (i, r["outcome"])
+        if r["outcome"] != "dense":
+            continue
+        n_dense += 1
+        o = oracle_mod.extract_depth(imgs[i], [imgs[k] for k in r["slots"]], r["T_slots"], cam,
+                                     p)
+        assert np.array_equal(b.get_debug(0), o["sparse"]), i
+        dense64 = oracle_mod.upsample(o["sparse"].astype(np.float64), imgs[i], p)
+        fused, new_seeds, _, _ = oracle_mod.fuse(dense64, seeds, r["T_fuse"], cam)
+        seeds = new_seeds.astype(np.float32)
+        depth = b.get_depth(0)
+        var = b.get_variance(0)
+        valid = fused > 0
+        n_oracle_valid += valid.sum()
+        assert (depth > 0).mean() == pytest.approx(valid.mean(), abs=2e-3), i
+        both = valid & (depth > 0)
+        n_valid += both.sum()
+        if both.any():
+            rel = np.abs(depth[both] - fused[both]) / fused[both]
+            worst_depth = max(worst_depth, float(np.percentile(rel, 99)))
+        # the variance of every seed the update wrote, valid or not
+        upd = new_seeds[..., 3] > 0
+        relv = np.abs(var[upd] - new_seeds[..., 3][upd]) / new_seeds[..., 3][upd]
+        worst_var = max(worst_var, float(np.percentile(relv, 99)))
+    assert n_dense >= 15
+    assert n_oracle_valid > 0
+    assert n_valid == pytest.approx(n_oracle_valid, rel=0.01, abs=50)
+    assert worst_depth < FUSE_RTOL and worst_var < FUSE_RTOL, (worst_depth, worst_var)
 
 
 def test_uneven_16_stream_batch_equals_single_streams(gpu):

@@ -30,10 +30,24 @@ def ref_lib():
     return refbuild
 
 
-def _slots(kf):
+def _slots(kf, n=5):
     from oracle.oracle import slots_from_ring
-    ks = slots_from_ring(5)
+    ks = slots_from_ring(n)
     return [kf.meas[k] for k in ks], kf.T_meas_ref[ks]
+
+
+def _assert_extract_equal(g, r, comp, W, H):
+    """Levels, cost volume, final BP messages, labels and sparse BP depths
+    bit for bit; upsampled depth within UPSAMPLE_RTOL."""
+    assert np.array_equal(g["levels"], r["levels"])
+    assert np.array_equal(g["cost"], r["cost"])
+    assert np.array_equal(g["messages"], r["messages"])
+    ref_labels = comp.labels_from_messages(r["cost"], r["messages"], r["levels"], W, H)
+    assert np.array_equal(g["labels"], ref_labels)
+    assert (ref_labels >= 0).sum() > 0
+    assert np.array_equal(g["sparse"], r["sparse"])
+    rel = np.abs(g["dense"] - r["dense"]) / np.abs(r["dense"])
+    assert rel.max() < UPSAMPLE_RTOL, rel.max()
 
 
 @pytest.mark.parametrize("W,H,stream", [(160, 128, 21), (752, 480, 22), (320, 240, 23)])
@@ -48,14 +62,42 @@ def test_extract_bit_exact_vs_reference_kernels(W, H, stream, ref_lib, gpu):
                              [torch.from_numpy(s).to(gpu) for s in slots], T, cam, p,
                              want_messages=True)
     g = {k: v.cpu().numpy() for k, v in g.items()}
-    assert np.array_equal(g["levels"], r["levels"])
-    assert np.array_equal(g["cost"], r["cost"])
-    assert np.array_equal(g["messages"], r["messages"])
-    ref_labels = ref_lib.labels_from_messages(r["cost"], r["messages"], r["levels"], W, H)
-    assert np.array_equal(g["labels"], ref_labels)
-    assert np.array_equal(g["sparse"], r["sparse"])
-    rel = np.abs(g["dense"] - r["dense"]) / np.abs(r["dense"])
-    assert rel.max() < UPSAMPLE_RTOL, rel.max()
+    _assert_extract_equal(g, r, ref_lib, W, H)
+
+
+# The measured configurations, against comparator builds of the reference's
+# kernels patched to their hypothesis count and range (oracle/refpatch.py):
+# the bench workload (752x480, fx = 460, 64 hypotheses over inverse depth
+# [1/50, 1/0.5], 5 slots) and the large keyframe (1920x1080, fx = 1150, 128
+# hypotheses over the same range).  The reference launches its cost kernel
+# with one thread per (hypothesis, slot) in one block (seed_matrix.cu:503-507),
+# so at 128 hypotheses at most 8 slots fit the 1024 threads of a block: 8 is
+# the largest slot count the reference itself can run there (the large
+# workload's 20 slots also exceed the kernel's 10-slot shared arrays,
+# depth_extract.cu:160).
+@pytest.mark.parametrize("variant,W,H,f,D,F,stream", [
+    ("d64_lo0.02", 752, 480, 460.0, 64, 5, 31),
+    ("d128_lo0.02", 1920, 1080, 1150.0, 128, 8, 32),
+])
+def test_measured_configs_bit_exact_vs_patched_reference(variant, W, H, f, D, F, stream, gpu):
+    from open_quadtree_mapping_b200 import stages
+    comp = refbuild.variant(variant)
+    if not comp.available():
+        pytest.skip("patched comparator %s not built (make -C oracle ref-variants)" % variant)
+    p = Params.for_range(D, 0.5, 50.0, arith=ARITH_REFERENCE)
+    # the library's parameters are the patched build's constants, bit for bit
+    assert comp.depth_num == D
+    assert p.min_inv_depth == comp.min_inv_depth
+    assert p.inv_depth_step == comp.inv_depth_step
+    kf = keyframe(stream, W, H, 11, f)
+    cam = cam_of(kf)
+    r = comp.extract(kf.ref, kf.meas, kf.T_meas_ref, cam, nslots=F)
+    slots, T = _slots(kf, F)
+    g = stages.extract_depth(torch.from_numpy(kf.ref).to(gpu),
+                             [torch.from_numpy(s).to(gpu) for s in slots], T, cam, p,
+                             want_messages=True)
+    g = {k: v.cpu().numpy() for k, v in g.items()}
+    _assert_extract_equal(g, r, refbuild, W, H)
 
 
 def test_fuse_vs_reference_kernels(ref_lib, oracle_mod, gpu):

@@ -77,6 +77,32 @@ def test_no_alloc_matches_workspace_entry(W, H, arith, gpu):
     assert not np.array_equal(outs[0], outs[1])
 
 
+def test_no_alloc_calls_leave_free_device_memory_unchanged(gpu):
+    """After a first call (the per-device set-up), back-to-back calls on one
+    stream allocate no device memory: the driver's free-memory count stays
+    the same.  The workspace entry's reference output is computed after the
+    loop, so nothing else allocates in between."""
+    dev = gpu
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    params = Params(arith=ARITH_IEEE)
+    W, H = 752, 480
+    img_h, sparse_h = _case(W, H, 7)
+    img = torch.from_numpy(img_h).to(dev)
+    sparse = torch.from_numpy(sparse_h).to(dev)
+    dense = torch.empty((H, W), dtype=torch.float32, device=dev)
+    assert _no_alloc(sparse, img, params, dense, stream) == 0, _lib.lib().qm_last_error()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(8):
+        assert _no_alloc(sparse, img, params, dense, stream) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    got = dense.cpu().numpy()
+    want = _with_workspace(sparse, img, params, stream).cpu().numpy()
+    np.testing.assert_allclose(got, want, rtol=RTOL, atol=0)
+
+
 def test_no_alloc_rejects_oversize_and_bad_shapes(gpu):
     dev = gpu
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
