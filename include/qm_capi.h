@@ -207,6 +207,14 @@ int qm_batch_set_branches(qm_batch *b, int branches);
  * it, so the range's half-sweeps hit L2.  0 = every level over all streams
  * at once (the default).  Results do not depend on it. */
 int qm_batch_set_group_bytes(qm_batch *b, size_t bytes);
+/* Coarse BP levels in one launch: the top pyramid levels with at most
+ * max_cells cells in every stream (and at least two half-sweeps) run all
+ * their half-sweeps in one launch, a cluster of blocks per stream with a
+ * hardware cluster barrier between half-sweeps, instead of one launch per
+ * half-sweep as the reference's bp_extract (bpextract.cu:122-143).  0 = one
+ * launch per half-sweep everywhere; default 4096.  Results do not depend on
+ * it. */
+int qm_batch_set_coarse_bp(qm_batch *b, int max_cells);
 /* Launch shapes of the BP and line-solver kernels: warps per block of the
  * BP half-sweeps and of the extraction (4, 8 or 16), rows per block of the
  * row solve (1, 2 or 4) and columns per block of the column solve (2, 4 or
@@ -390,6 +398,18 @@ int qm_bp_soft_backward(const float *cost, int width, int height, const uint8_t 
                         const qm_params *p, float tau, const float *grad_sparse,
                         double *grad_penalties, void *workspace, size_t workspace_bytes,
                         void *stream);
+/* The soft BP of qm_bp_soft_* in FP64 throughout (data terms, messages, the
+ * readout and the adjoint), for checking gradients against FP64 finite
+ * differences; the FP32 entry points above are the fitting path.  Same
+ * arguments; the workspace (qm_bp_soft64_workspace_size) is its own. */
+int qm_bp_soft64_workspace_size(int width, int height, const qm_params *p, size_t *bytes);
+int qm_bp_soft64_forward(const float *cost, int width, int height, const uint8_t *levels,
+                         const qm_params *p, float tau, float *sparse, void *workspace,
+                         size_t workspace_bytes, void *stream);
+int qm_bp_soft64_backward(const float *cost, int width, int height, const uint8_t *levels,
+                          const qm_params *p, float tau, const float *grad_sparse,
+                          double *grad_penalties, void *workspace, size_t workspace_bytes,
+                          void *stream);
 /* Upsampling with a weight factor per pixel: the systems of qm_upsample with
  * every inner edge weight (between a pixel and its left or upper neighbour)
  * multiplied by omega at that pixel, solved per line in FP64.  The backward

@@ -88,6 +88,7 @@ _SIGS = {
     "qm_batch_set_branches": (_I, [_P, _I]),
     "qm_depthmap_set_semidense": (_I, [_P, _I]),
     "qm_batch_set_group_bytes": (_I, [_P, _S]),
+    "qm_batch_set_coarse_bp": (_I, [_P, _I]),
     "qm_batch_set_autotune": (_I, [_P, _I]),
     "qm_batch_set_tune": (_I, [_P, ctypes.POINTER(_I)]),
     "qm_batch_get_tune": (_I, [_P, ctypes.POINTER(_I)]),
@@ -114,6 +115,10 @@ _SIGS = {
     "qm_bp_soft_workspace_size": (_I, [_I, _I, ctypes.POINTER(QmParamsC), ctypes.POINTER(_S)]),
     "qm_bp_soft_forward": (_I, [_P, _I, _I, _P, ctypes.POINTER(QmParamsC), _F, _P, _P, _S, _P]),
     "qm_bp_soft_backward": (_I, [_P, _I, _I, _P, ctypes.POINTER(QmParamsC), _F, _P, _P, _P, _S,
+                                 _P]),
+    "qm_bp_soft64_workspace_size": (_I, [_I, _I, ctypes.POINTER(QmParamsC), ctypes.POINTER(_S)]),
+    "qm_bp_soft64_forward": (_I, [_P, _I, _I, _P, ctypes.POINTER(QmParamsC), _F, _P, _P, _S, _P]),
+    "qm_bp_soft64_backward": (_I, [_P, _I, _I, _P, ctypes.POINTER(QmParamsC), _F, _P, _P, _P, _S,
                                  _P]),
     "qm_upsample_w_workspace_size": (_I, [_I, _I, ctypes.POINTER(_S)]),
     "qm_upsample_w_forward": (_I, [_P, _P, _S, _I, _I, ctypes.POINTER(QmParamsC), _P, _P, _P,

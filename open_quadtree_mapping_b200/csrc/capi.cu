@@ -330,6 +330,195 @@ struct SoftBp
   }
 };
 
+// The gradient-check mode of the soft BP: the same forward and adjoint with
+// every data term, message, state snapshot and adjoint in FP64 (the product
+// path's BP is FP32).  Workspace: per level the FP64 data term (level 0
+// widened from the FP32 cost) and four message images, the largest level's
+// (iterations + 1) state snapshots, and two adjoint buffers of level 0's
+// size.
+struct SoftLayout64
+{
+  size_t lv = 0, hist = 0, dir = 0, total = 0;
+};
+
+SoftLayout64 soft_layout64(int W, int H, const qm_params &p)
+{
+  SoftLayout64 L;
+  int w = W / 4, h = H / 4;
+  L.dir = align256((size_t)w * h * p.num_hyp * sizeof(double));
+  for (int l = 0; l < p.bp_levels; ++l)
+  {
+    const size_t n = align256((size_t)w * h * p.num_hyp * sizeof(double));
+    L.lv += 5 * n;
+    L.hist = std::max(L.hist, (size_t)(p.bp_iters[l] + 1) * 4 * n);
+    w = (w + 1) / 2;
+    h = (h + 1) / 2;
+  }
+  L.total = L.lv + L.hist + 2 * 4 * L.dir;
+  return L;
+}
+
+struct SoftBp64
+{
+  int W, H, D, L;
+  const uint8_t *levels;
+  const float *cost;
+  SoftLayout64 lay;
+  int lw[qm::kMaxLevels], lh[qm::kMaxLevels];
+  double *data[qm::kMaxLevels];
+  qm::MsgPtrs64 msg[qm::kMaxLevels];
+  char *hist = nullptr, *adj[2] = {nullptr, nullptr};
+
+  SoftBp64(const float *cost_, int W_, int H_, const uint8_t *levels_, const qm_params &q,
+           void *ws, size_t bytes)
+      : W(W_), H(H_), D(q.num_hyp), L(q.bp_levels), levels(levels_), cost(cost_)
+  {
+    lay = soft_layout64(W, H, q);
+    if (!ws || bytes < lay.total)
+      throw CudaError{QM_ERR_WORKSPACE, "soft BP (FP64) workspace too small"};
+    require(((uintptr_t)cost | (uintptr_t)ws) % 16 == 0,
+            "cost and workspace must be 16-byte aligned");
+    char *b = (char *)ws;
+    size_t o = 0;
+    int w = W / 4, h = H / 4;
+    for (int l = 0; l < L; ++l)
+    {
+      const size_t n = align256((size_t)w * h * D * sizeof(double));
+      lw[l] = w;
+      lh[l] = h;
+      data[l] = (double *)(b + o);
+      o += n;
+      for (int m = 0; m < 4; ++m)
+      {
+        msg[l].m[m] = (double *)(b + o);
+        o += n;
+      }
+      w = (w + 1) / 2;
+      h = (h + 1) / 2;
+    }
+    hist = b + lay.lv;
+    adj[0] = hist + lay.hist;
+    adj[1] = adj[0] + 4 * lay.dir;
+  }
+
+  qm::DiffBp64 level_args(int l, const qm_params &q, float tau) const
+  {
+    qm::DiffBp64 a;
+    std::memset(&a, 0, sizeof(a));
+    a.W = W;
+    a.H = H;
+    a.D = D;
+    a.w = lw[l];
+    a.h = lh[l];
+    a.level = l;
+    a.qt_max = q.qt_max_level;
+    a.levels = levels;
+    a.data = data[l];
+    for (int m = 0; m < 4; ++m)
+      a.S[m] = msg[l].m[m];
+    a.P1 = q.P1;
+    a.P2 = q.P2;
+    a.tau = tau;
+    a.step = q.inv_depth_step;
+    a.min_inv = q.min_inv_depth;
+    return a;
+  }
+
+  qm::MsgPtrs64 adjoint(int buf) const
+  {
+    qm::MsgPtrs64 p;
+    for (int m = 0; m < 4; ++m)
+      p.m[m] = (double *)(adj[buf] + m * lay.dir);
+    return p;
+  }
+
+  // every cell of level l from its parent's final messages, then the
+  // level's half-sweeps; snap(i) after the start and after every half-sweep
+  template <class Snap>
+  void sweep_level(int l, const qm_params &q, Snap &&snap, cudaStream_t s)
+  {
+    qm::launch_msg_inherit_all64(l + 1 < L ? &msg[l + 1] : nullptr, l + 1 < L ? lw[l + 1] : 0,
+                                 msg[l], lw[l], lh[l], D, s);
+    snap(0);
+    for (int i = 0; i < q.bp_iters[l]; ++i)
+    {
+      qm::DiffBp64 a = level_args(l, q, 0.0f);
+      a.parity = i & 1;
+      qm::launch_bp_sweep_fwd64(a, msg[l], s);
+      snap(i + 1);
+    }
+  }
+
+  void forward(const qm_params &q, float tau, float *sparse, cudaStream_t s)
+  {
+    qm::launch_widen(cost, data[0], (long)lw[0] * lh[0] * D, s);
+    for (int l = 1; l < L; ++l)
+      qm::launch_pyramid64(data[l - 1], lw[l - 1], lh[l - 1], data[l], lw[l], lh[l], D, s);
+    for (int l = L - 1; l >= 0; --l)
+      sweep_level(l, q, [](int) {}, s);
+    qm::check(cudaMemsetAsync(sparse, 0, sizeof(float) * W * H, s), "memset");
+    qm::DiffBp64 a = level_args(0, q, tau);
+    a.sparse = sparse;
+    qm::launch_soft_readout(a, 0, s);
+    qm::check(cudaGetLastError(), "soft BP (FP64)");
+  }
+
+  // as SoftBp::backward, in FP64
+  void backward(const qm_params &q, float tau, const float *g_sparse, double *gP,
+                cudaStream_t s)
+  {
+    qm::check(cudaMemsetAsync(gP, 0, 2 * sizeof(double), s), "memset");
+    int cur = 0;
+    qm::check(cudaMemsetAsync(adj[cur], 0, 4 * lay.dir, s), "memset");
+    {
+      qm::DiffBp64 a = level_args(0, q, tau);
+      const qm::MsgPtrs64 A = adjoint(cur);
+      for (int m = 0; m < 4; ++m)
+        a.A[m] = A.m[m];
+      a.g_sparse = g_sparse;
+      qm::launch_soft_readout(a, 1, s);
+    }
+    for (int l = 0; l < L; ++l)
+    {
+      const size_t n = (size_t)lw[l] * lh[l] * D;
+      const size_t slot = align256(n * sizeof(double));
+      auto state = [&](int i, int m) { return (double *)(hist + ((size_t)i * 4 + m) * slot); };
+      sweep_level(l, q,
+                  [&](int i) {
+                    for (int m = 0; m < 4; ++m)
+                      qm::check(cudaMemcpyAsync(state(i, m), msg[l].m[m], n * sizeof(double),
+                                                cudaMemcpyDeviceToDevice, s),
+                                "message snapshot");
+                  },
+                  s);
+      const qm::MsgPtrs64 A = adjoint(cur);
+      for (int i = q.bp_iters[l] - 1; i >= 0; --i)
+      {
+        qm::DiffBp64 a = level_args(l, q, tau);
+        for (int m = 0; m < 4; ++m)
+        {
+          a.S[m] = state(i, m);
+          a.A[m] = A.m[m];
+        }
+        a.parity = i & 1;
+        a.gP = gP;
+        qm::launch_bp_sweep_bwd(a, s);
+      }
+      if (l + 1 < L)
+      {
+        const qm::MsgPtrs64 P = adjoint(cur ^ 1);
+        for (int m = 0; m < 4; ++m)
+          qm::check(cudaMemsetAsync(P.m[m], 0, (size_t)lw[l + 1] * lh[l + 1] * D * sizeof(double),
+                                    s),
+                    "memset");
+        qm::launch_msg_downsample_add(A, lw[l], lh[l], P, lw[l + 1], lh[l + 1], D, s);
+        cur ^= 1;
+      }
+    }
+    qm::check(cudaGetLastError(), "soft BP (FP64) adjoint");
+  }
+};
+
 qm::DiffUp upw_args(const uint8_t *img, size_t pitch, int W, int H, const qm_params *p,
                     const float *omega, void *ws, size_t bytes)
 {
@@ -676,6 +865,16 @@ int qm_batch_set_group_bytes(qm_batch *b, size_t bytes)
   return guarded([&] {
     require(b != nullptr, "NULL handle");
     b->set->engine().set_group_bytes(bytes);
+  });
+}
+
+int qm_batch_set_coarse_bp(qm_batch *b, int max_cells)
+{
+  return guarded([&] {
+    require(b != nullptr, "NULL handle");
+    require(max_cells >= 0, "max_cells must be >= 0");
+    std::lock_guard<std::mutex> lock(b->set->mutex());
+    b->set->engine().set_coarse_cells(max_cells);
   });
 }
 
@@ -1094,6 +1293,43 @@ int qm_bp_soft_backward(const float *cost, int width, int height, const uint8_t 
             "NULL argument or tau <= 0");
     const qm_params q = params_or_default(p);
     SoftBp sb(cost, width, height, levels, q, workspace, workspace_bytes);
+    sb.backward(q, tau, grad_sparse, grad_penalties, as_stream(stream));
+  });
+}
+
+int qm_bp_soft64_workspace_size(int width, int height, const qm_params *p, size_t *bytes)
+{
+  return guarded([&] {
+    check_stage_size(width, height);
+    require(bytes != nullptr, "NULL argument");
+    *bytes = soft_layout64(width, height, params_or_default(p)).total;
+  });
+}
+
+int qm_bp_soft64_forward(const float *cost, int width, int height, const uint8_t *levels,
+                         const qm_params *p, float tau, float *sparse, void *workspace,
+                         size_t workspace_bytes, void *stream)
+{
+  return guarded([&] {
+    check_stage_size(width, height);
+    require(cost && levels && sparse && tau > 0.0f, "NULL argument or tau <= 0");
+    const qm_params q = params_or_default(p);
+    SoftBp64 sb(cost, width, height, levels, q, workspace, workspace_bytes);
+    sb.forward(q, tau, sparse, as_stream(stream));
+  });
+}
+
+int qm_bp_soft64_backward(const float *cost, int width, int height, const uint8_t *levels,
+                          const qm_params *p, float tau, const float *grad_sparse,
+                          double *grad_penalties, void *workspace, size_t workspace_bytes,
+                          void *stream)
+{
+  return guarded([&] {
+    check_stage_size(width, height);
+    require(cost && levels && grad_sparse && grad_penalties && tau > 0.0f,
+            "NULL argument or tau <= 0");
+    const qm_params q = params_or_default(p);
+    SoftBp64 sb(cost, width, height, levels, q, workspace, workspace_bytes);
     sb.backward(q, tau, grad_sparse, grad_penalties, as_stream(stream));
   });
 }

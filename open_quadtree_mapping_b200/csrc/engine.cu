@@ -86,6 +86,7 @@ struct StageTable
   std::vector<int> uniform;        // per stage: blocks per job when all agree, else 0
   std::vector<int> dvals;          // hypothesis counts present
   std::vector<size_t> level_bytes; // per job and BP level: data + messages
+  std::vector<long> level_cells;   // per BP level: largest cell count over the jobs
   int max_w = 0, max_h = 0;        // longest lines of the row / column solves
   Tune tune;                       // launch shapes the blocks were counted for
 
@@ -139,8 +140,8 @@ std::vector<int> job_groups(const StageTable &T, int level, int L, size_t budget
 // all).  When `prof` is given, every launch is bracketed by a pair of events
 // recorded on `s`.  Returns the number of kernel launches.
 int enqueue_range(const Batch &B, const StageTable &T, const qm_params &p, size_t group_bytes,
-                  int first, int last, cudaStream_t s, LaunchProfile *prof = nullptr, int ja = 0,
-                  int jb = -1)
+                  int coarse_cells, int first, int last, cudaStream_t s,
+                  LaunchProfile *prof = nullptr, int ja = 0, int jb = -1)
 {
   if (jb < 0)
     jb = T.n;
@@ -189,8 +190,26 @@ int enqueue_range(const Batch &B, const StageTable &T, const qm_params &p, size_
   all(kCost, st.cost(), [&](const Batch &b, int g) { launch_cost(b, g, ar, max_d, s); });
   for (int l = 1; l < L; ++l)
     all(kPyramid, st.pyr(l), [&](const Batch &b, int g) { launch_pyramid(b, g, l, s); });
-  // BP, coarse to fine; each level runs job range by job range (message
-  // inheritance, half-sweeps, and at level 0 the extraction)
+  // BP, coarse to fine.  The top levels lc..L-1 whose cells are few (and
+  // which have two or more half-sweeps) run as one cluster launch per
+  // hypothesis count; below them each level runs job range by job range
+  // (message inheritance, half-sweeps, and at level 0 the extraction)
+  int lc = L;
+  if (coarse_cells > 0 && (int)T.level_cells.size() == L)
+    while (lc > 0 && p.bp_iters[lc - 1] >= 2 && T.level_cells[lc - 1] <= coarse_cells &&
+           in(st.sweep(lc - 1)))
+      --lc;
+  if (lc < L && jb > ja)
+  {
+    CoarsePlan cp;
+    std::memset(&cp, 0, sizeof(cp));
+    cp.lo = lc;
+    cp.hi = L - 1;
+    for (int l = 0; l < L; ++l)
+      cp.iters[l] = p.bp_iters[l];
+    for (int d : T.dvals)
+      launch(kSweep, [&] { launch_bp_coarse(B, ja, jb - ja, d, cp, kp, ar, s); });
+  }
   for (int l = L - 1; l >= 0; --l)
   {
     const std::vector<int> groups = job_groups(T, l, L, group_bytes, ja, jb);
@@ -201,7 +220,9 @@ int enqueue_range(const Batch &B, const StageTable &T, const qm_params &p, size_
       // with two or more half-sweeps the first two write the inherited
       // messages themselves (no separate pass)
       const bool fold = p.bp_iters[l] >= 2;
-      if (!fold && in(st.inherit(l)))
+      if (l >= lc)
+        ; // swept by the coarse launch
+      else if (!fold && in(st.inherit(l)))
       {
         const Batch b = at(st.inherit(l), j0, j1, grid);
         if (grid > 0)
@@ -209,7 +230,7 @@ int enqueue_range(const Batch &B, const StageTable &T, const qm_params &p, size_
             launch_msg_inherit(b, grid, l, p.bp_iters[l], p.qt_max_level, s);
           });
       }
-      if (in(st.sweep(l)))
+      if (l < lc && in(st.sweep(l)))
       {
         const Batch b = at(st.sweep(l), j0, j1, grid);
         if (grid > 0)
@@ -441,6 +462,7 @@ struct Plan
   std::unique_ptr<TableBuf> tb;
   bool tuned = false;                  // launch shapes settled (timed or fixed)
   size_t group_bytes = 0;              // the job grouping the graphs were captured with
+  int coarse_cells = 0;                // the coarse-level threshold they were captured with
   cudaGraphExec_t exec[2] = {nullptr, nullptr}; // by step parity
   StageTable &table() { return tb->table; }
   void drop_graphs()
@@ -665,6 +687,9 @@ std::unique_ptr<TableBuf> Engine::build_table(const std::vector<int> &active, co
     for (int l = 0; l < L; ++l)
       T.level_bytes.push_back((size_t)5 * layouts_[j].lw[l] * layouts_[j].lh[l] * shapes_[j].D *
                               sizeof(float));
+    T.level_cells.resize(L, 0);
+    for (int l = 0; l < L; ++l)
+      T.level_cells[l] = std::max(T.level_cells[l], (long)layouts_[j].lw[l] * layouts_[j].lh[l]);
   }
   T.add_jobs(per_job, ds);
   const int ns = (int)T.uniform.size();
@@ -683,7 +708,7 @@ Plan &Engine::plan_for(const std::vector<int> &active)
   if (it != plans_.end())
   {
     Plan &pl = *it->second;
-    if (pl.group_bytes != group_bytes_)
+    if (pl.group_bytes != group_bytes_ || pl.coarse_cells != coarse_cells_)
       pl.drop_graphs();
     return pl;
   }
@@ -749,7 +774,8 @@ void Engine::tune_plan(Plan &pl)
     float ms[kNumKinds] = {};
     try
     {
-      enqueue_range(B, cand[c]->table, params_, group_bytes_, 0, st.count() - 1, stream_, &prof);
+      enqueue_range(B, cand[c]->table, params_, group_bytes_, coarse_cells_, 0, st.count() - 1,
+                    stream_, &prof);
       check(cudaStreamSynchronize(stream_), "autotune run");
     }
     catch (...)
@@ -870,10 +896,12 @@ int Engine::enqueue(Plan &pl, cudaStream_t s)
   const Batch B = upload((int)pl.active.size(), s);
   const Stages st{params_.bp_levels};
   pl.group_bytes = group_bytes_;
+  pl.coarse_cells = coarse_cells_;
   const int n = (int)pl.active.size();
   const int k = std::min(branches_, n);
   if (k < 2)
-    return enqueue_range(B, pl.table(), params_, group_bytes_, 0, st.count() - 1, s);
+    return enqueue_range(B, pl.table(), params_, group_bytes_, coarse_cells_, 0, st.count() - 1,
+                         s);
   // k independent branches over consecutive ranges of the jobs (every stage
   // is per job): the GPU fills the latency-bound stretches of one branch
   // (coarse BP levels, line solves) with the other branches' work
@@ -884,8 +912,8 @@ int Engine::enqueue(Plan &pl, cudaStream_t s)
     cudaStream_t bs = i == 0 ? s : branch_[i - 1];
     if (i > 0)
       check(cudaStreamWaitEvent(bs, ev_fork_, 0), "fork");
-    nl += enqueue_range(B, pl.table(), params_, group_bytes_, 0, st.count() - 1, bs, nullptr,
-                        n * i / k, n * (i + 1) / k);
+    nl += enqueue_range(B, pl.table(), params_, group_bytes_, coarse_cells_, 0, st.count() - 1,
+                        bs, nullptr, n * i / k, n * (i + 1) / k);
   }
   for (int i = 1; i < k; ++i)
   {
@@ -972,7 +1000,8 @@ void Engine::profile(const std::vector<int> &active, float *ms, int *launches)
   LaunchProfile prof;
   try
   {
-    enqueue_range(B, pl.table(), params_, group_bytes_, 0, st.count() - 1, stream_, &prof);
+    enqueue_range(B, pl.table(), params_, group_bytes_, coarse_cells_, 0, st.count() - 1, stream_,
+                  &prof);
     check(cudaStreamSynchronize(stream_), "profile run");
   }
   catch (...)
@@ -1026,7 +1055,9 @@ int run_range(const Batch &B, const Shape &s, const qm_params &p, int first, int
   T.add_jobs({stage_blocks(s, lay, p, T.tune)}, {s.D});
   T.max_w = s.W;
   T.max_h = s.H;
-  return enqueue_range(B, T, p, 0, first, last, stream);
+  for (int l = 0; l < p.bp_levels; ++l)
+    T.level_cells.push_back((long)lay.lw[l] * lay.lh[l]);
+  return enqueue_range(B, T, p, 0, QM_DEFAULT_COARSE_CELLS, first, last, stream);
 }
 
 int first_of(const char *name, int L)

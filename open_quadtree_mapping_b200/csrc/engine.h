@@ -59,6 +59,16 @@ constexpr size_t kDefaultGroupBytes = 0;
 // of the active jobs as independent graph branches) measured 3 % faster than
 // one sequence at 32 streams of 752x480 (3.27 vs 3.37 ms per batch), with
 // bit-identical results.
+// Default coarse-level threshold of the BP: the top pyramid levels whose
+// largest cell count over the active jobs is at most this run all their
+// half-sweeps in one cluster launch (k_bp_coarse) instead of one launch per
+// half-sweep; 0 disables it.  4096 takes levels 2 and 3 of a 752x480 or
+// 1280x720 keyframe (1410 / 360 and 3600 / 920 cells) and level 3 of a
+// 1920x1080 one.
+#ifndef QM_DEFAULT_COARSE_CELLS
+#define QM_DEFAULT_COARSE_CELLS 4096
+#endif
+
 #ifndef QM_DEFAULT_BRANCHES
 #define QM_DEFAULT_BRANCHES 2
 #endif
@@ -180,6 +190,11 @@ public:
   void set_branches(int k);
   int branches() const { return branches_; }
   size_t group_bytes() const { return group_bytes_; }
+  // coarse BP levels (at most `cells` cells in every active job) in one
+  // cluster launch; 0: one launch per half-sweep at every level.  Results
+  // do not depend on it.
+  void set_coarse_cells(int cells) { coarse_cells_ = cells < 0 ? 0 : cells; }
+  int coarse_cells() const { return coarse_cells_; }
   int last_launches() const { return last_launches_; }
   // 1: the sparse buffers arrive filled with the semi-dense tracker's depths
   // (the quadtree pass keeps them instead of clearing)
@@ -242,6 +257,7 @@ private:
   bool graphs_ = true;
   int parity_ = 0;
   size_t group_bytes_ = kDefaultGroupBytes;
+  int coarse_cells_ = QM_DEFAULT_COARSE_CELLS;
   int last_launches_ = 0;
   bool autotune_ = true;
   Tune fixed_tune_, last_tune_;

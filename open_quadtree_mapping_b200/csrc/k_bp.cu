@@ -266,23 +266,31 @@ __global__ void __launch_bounds__(kFlatThreads)
 // bp kernel (bpextract.cu:200-312), one lane group per cell of the active
 // colour.  Groups whose cell is skipped or out of range still take part in
 // the warp's shuffles (full masks) with zero inputs and store nothing.
-template <int D, int ARITH>
-__global__ void __launch_bounds__(kMaxCellWarps * 32, 4)
-    k_bp_sweep(const __grid_constant__ Batch B, int level, int parity, int first, int inherit,
-               KParams kp)
+//
+// msg_load: messages another block of the same launch may have written since
+// the launch began are read through L2 (ld.global.cg) by the coarse-level
+// kernel below, whose blocks hand messages to each other across cluster
+// barriers; the one-launch-per-half-sweep kernel reads them normally.
+template <bool L2_ONLY>
+__device__ __forceinline__ float msg_load(const float *p)
+{
+  if constexpr (L2_ONLY)
+    return __ldcg(p);
+  else
+    return *p;
+}
+
+// One warp's lane groups of half-sweep `parity` at `level`: items item0 ..
+// item0 + G - 1 of the colour's cells (item = y * ceil(w / 2) + x / 2).
+template <int D, int ARITH, bool L2_ONLY>
+__device__ __forceinline__ void sweep_warp(const JobDesc &J, int level, int parity, int first,
+                                           int inherit, const KParams &kp, int item0)
 {
   using HL = HypLayout<D>;
-  constexpr int NV = HL::NV, LPC = HL::LPC, G = HL::G;
-  int lb;
-  const JobDesc &J = job_of(B, lb);
-  if (J.D != D)
-    return;
+  constexpr int NV = HL::NV, LPC = HL::LPC;
   const LevelDesc &L = J.lv[level];
   const int w = L.w, h = L.h, hw = (w + 1) / 2;
   const int lane = threadIdx.x & 31, gl = lane & (LPC - 1);
-  const int item0 = (lb * (int)(blockDim.x >> 5) + (threadIdx.x >> 5)) * G;
-  if (item0 >= hw * h)
-    return; // the whole warp
   const int item = item0 + lane / LPC;
   int x = 0, y = 0;
   bool act = item < hw * h, skipped = false;
@@ -310,7 +318,7 @@ __global__ void __launch_bounds__(kMaxCellWarps * 32, 4)
       for (int k = 0; k < NV; ++k)
       {
         const int d = gl + LPC * k;
-        L.msg[m][c * D + d] = top ? 0.0f : C.msg[m][pc + d];
+        L.msg[m][c * D + d] = top ? 0.0f : msg_load<L2_ONLY>(C.msg[m] + pc + d);
       }
   }
   if (!__any_sync(0xffffffffu, act))
@@ -347,10 +355,10 @@ __global__ void __launch_bounds__(kMaxCellWarps * 32, 4)
   {
     const int d = gl + LPC * k;
     dat[k] = act ? L.data[c * D + d] : 0.0f;
-    fu[k] = (ld && has_u) ? src_u[d] : 0.0f;
-    fd[k] = (ld && has_d) ? src_d[d] : 0.0f;
-    fl[k] = (ld && has_l) ? src_l[d] : 0.0f;
-    fr[k] = (ld && has_r) ? src_r[d] : 0.0f;
+    fu[k] = (ld && has_u) ? msg_load<L2_ONLY>(src_u + d) : 0.0f;
+    fd[k] = (ld && has_d) ? msg_load<L2_ONLY>(src_d + d) : 0.0f;
+    fl[k] = (ld && has_l) ? msg_load<L2_ONLY>(src_l + d) : 0.0f;
+    fr[k] = (ld && has_r) ? msg_load<L2_ONLY>(src_r + d) : 0.0f;
   }
   const float P1 = kp.P1, P2 = kp.P2;
   // h of every direction: the data term plus the three other incoming
@@ -410,6 +418,63 @@ __global__ void __launch_bounds__(kMaxCellWarps * 32, 4)
 #pragma unroll
       for (int k = 0; k < NV; ++k)
         out[gl + LPC * k] = m[k] - mean;
+    }
+  }
+}
+
+template <int D, int ARITH>
+__global__ void __launch_bounds__(kMaxCellWarps * 32, 4)
+    k_bp_sweep(const __grid_constant__ Batch B, int level, int parity, int first, int inherit,
+               KParams kp)
+{
+  constexpr int G = HypLayout<D>::G;
+  int lb;
+  const JobDesc &J = job_of(B, lb);
+  if (J.D != D)
+    return;
+  const LevelDesc &L = J.lv[level];
+  const int hw = (L.w + 1) / 2;
+  const int item0 = (lb * (int)(blockDim.x >> 5) + (threadIdx.x >> 5)) * G;
+  if (item0 >= hw * L.h)
+    return; // the whole warp
+  sweep_warp<D, ARITH, false>(J, level, parity, first, inherit, kp, item0);
+}
+
+// Every half-sweep of the coarse levels lo..hi (coarse to fine) in one
+// launch: a cluster of kCoarseCtas blocks per job walks the levels, each
+// half-sweep spread over the cluster's warps, with a cluster barrier (a
+// hardware barrier: release / acquire at cluster scope, no spinning) between
+// half-sweeps.  A coarse level's costs and messages (about 2.3 MB per
+// 752x480 job at levels 2 and 3 together) stay in L2 across its sweeps, and
+// its 10 half-sweeps no longer pay a launch and a grid drain each.  The
+// arithmetic is the per-half-sweep kernel's (the same device function), so
+// the messages are bit-identical; messages are read through L2 because other
+// blocks of the cluster wrote them.  Every block of a cluster takes the same
+// barriers: the trip counts depend only on the job and the plan.
+template <int D, int ARITH>
+__global__ void __cluster_dims__(kCoarseCtas, 1, 1) __launch_bounds__(kCoarseThreads, 2)
+    k_bp_coarse(const __grid_constant__ Batch B, int j0, CoarsePlan plan, KParams kp)
+{
+  constexpr int G = HypLayout<D>::G;
+  const int job = j0 + (int)blockIdx.x / kCoarseCtas;
+  const JobDesc &J = B.jobs ? B.jobs[job] : B.one;
+  if (J.D != D)
+    return; // the whole cluster
+  const int warps = kCoarseThreads / 32;
+  const int gw = (int)(blockIdx.x % kCoarseCtas) * warps + (int)(threadIdx.x >> 5);
+  const int stride = kCoarseCtas * warps * G;
+  for (int level = plan.hi; level >= plan.lo; --level)
+  {
+    const LevelDesc &L = J.lv[level];
+    const int n = (L.w + 1) / 2 * L.h;
+    const int iters = plan.iters[level];
+    for (int it = 0; it < iters; ++it)
+    {
+      for (int item0 = gw * G; item0 < n; item0 += stride)
+        sweep_warp<D, ARITH, true>(J, level, it & 1, it == 0 ? 1 : 0, it < 2 ? 1 : 0, kp,
+                                   item0);
+      asm volatile("barrier.cluster.arrive.release.aligned;\n"
+                   "barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
     }
   }
 }
@@ -534,6 +599,17 @@ void sweep_d(const Batch &B, int blocks, int level, int parity, int first, int i
 }
 
 template <int D>
+void coarse_d(const Batch &B, int j0, int jobs, const CoarsePlan &plan, KParams kp, int arith,
+              cudaStream_t s)
+{
+  if (arith == QM_ARITH_IEEE)
+    k_bp_coarse<D, QM_ARITH_IEEE><<<jobs * kCoarseCtas, kCoarseThreads, 0, s>>>(B, j0, plan, kp);
+  else
+    k_bp_coarse<D, QM_ARITH_REFERENCE>
+        <<<jobs * kCoarseCtas, kCoarseThreads, 0, s>>>(B, j0, plan, kp);
+}
+
+template <int D>
 void extract_d(const Batch &B, int blocks, int arith, int warps, cudaStream_t s)
 {
   if (arith == QM_ARITH_IEEE)
@@ -601,6 +677,20 @@ void launch_bp_sweep_own(const Batch &B, int blocks, int d, int level, int parit
                          int arith, cudaStream_t s, int warps)
 {
   sweep_any(B, blocks, d, level, parity, 0, 0, kp, arith, warps, s);
+}
+
+void launch_bp_coarse(const Batch &B, int j0, int jobs, int d, const CoarsePlan &plan,
+                      KParams kp, int arith, cudaStream_t s)
+{
+  switch (d)
+  {
+  case 32: coarse_d<32>(B, j0, jobs, plan, kp, arith, s); break;
+  case 48: coarse_d<48>(B, j0, jobs, plan, kp, arith, s); break;
+  case 64: coarse_d<64>(B, j0, jobs, plan, kp, arith, s); break;
+  case 96: coarse_d<96>(B, j0, jobs, plan, kp, arith, s); break;
+  case 128: coarse_d<128>(B, j0, jobs, plan, kp, arith, s); break;
+  default: break;
+  }
 }
 
 void launch_extract(const Batch &B, int blocks, int d, int arith, cudaStream_t s, int warps)

@@ -46,7 +46,27 @@ namespace
 
 constexpr int kDiffWarps = 8;
 
-__device__ __forceinline__ float warp_sum_f(float v)
+// Arithmetic of a real type: float for the product path, double for the
+// gradient-check mode.
+template <class R>
+struct Real;
+template <>
+struct Real<float>
+{
+  static __device__ __forceinline__ float big() { return FLT_MAX; }
+  static __device__ __forceinline__ float min(float a, float b) { return fminf(a, b); }
+  static __device__ __forceinline__ float exp(float a) { return expf(a); }
+};
+template <>
+struct Real<double>
+{
+  static __device__ __forceinline__ double big() { return DBL_MAX; }
+  static __device__ __forceinline__ double min(double a, double b) { return fmin(a, b); }
+  static __device__ __forceinline__ double exp(double a) { return ::exp(a); }
+};
+
+template <class R>
+__device__ __forceinline__ R warp_sum(R v)
 {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1)
@@ -54,36 +74,29 @@ __device__ __forceinline__ float warp_sum_f(float v)
   return v;
 }
 
-__device__ __forceinline__ double warp_sum_d(double v)
+template <class R>
+__device__ __forceinline__ R warp_min(R v)
 {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1)
-    v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
-__device__ __forceinline__ float warp_min_f(float v)
-{
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1)
-    v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    v = Real<R>::min(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
 }
 
 // value at hypothesis d-1 / d+1 of a per-lane register array (lane l holds
 // d = l + 32k), one shuffle per register; lanes at the ends of the range get
 // their own value back (callers mask them)
-template <int NV>
-__device__ __forceinline__ void neighbours(const float (&v)[NV], int lane, int k, float &prev,
-                                           float &next)
+template <int NV, class R>
+__device__ __forceinline__ void neighbours(const R (&v)[NV], int lane, int k, R &prev, R &next)
 {
-  const float up_src = (lane == 31 && k > 0) ? v[k > 0 ? k - 1 : 0] : v[k];
-  const float dn_src = (lane == 0 && k + 1 < NV) ? v[k + 1 < NV ? k + 1 : k] : v[k];
+  const R up_src = (lane == 31 && k > 0) ? v[k > 0 ? k - 1 : 0] : v[k];
+  const R dn_src = (lane == 0 && k + 1 < NV) ? v[k + 1 < NV ? k + 1 : k] : v[k];
   prev = __shfl_sync(0xffffffffu, up_src, (lane + 31) & 31);
   next = __shfl_sync(0xffffffffu, dn_src, (lane + 1) & 31);
 }
 
-__device__ __forceinline__ bool skipped(const DiffBp &a, int x, int y)
+template <class R>
+__device__ __forceinline__ bool skipped(const DiffBpR<R> &a, int x, int y)
 {
   const int ilev = a.level + 2;
   if (ilev > a.qt_max)
@@ -93,7 +106,8 @@ __device__ __forceinline__ bool skipped(const DiffBp &a, int x, int y)
   return (int)a.levels[(size_t)sy * a.W + sx] > ilev;
 }
 
-__device__ __forceinline__ bool is_node(const DiffBp &a, int x, int y)
+template <class R>
+__device__ __forceinline__ bool is_node(const DiffBpR<R> &a, int x, int y)
 {
   const int lvl = a.levels[(size_t)min(y * 4, a.H - 1) * a.W + min(x * 4, a.W - 1)];
   const int size = 1 << lvl;
@@ -101,9 +115,11 @@ __device__ __forceinline__ bool is_node(const DiffBp &a, int x, int y)
 }
 
 // ------------------------------------------------------------ soft readout
-template <int D>
-__global__ void __launch_bounds__(kDiffWarps * 32) k_soft_readout(const DiffBp a, int backward)
+template <int D, class R>
+__global__ void __launch_bounds__(kDiffWarps * 32)
+    k_soft_readout(const DiffBpR<R> a, int backward)
 {
+  using M = Real<R>;
   constexpr int NV = (D + 31) / 32;
   const int cell = blockIdx.x * kDiffWarps + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
@@ -114,12 +130,12 @@ __global__ void __launch_bounds__(kDiffWarps * 32) k_soft_readout(const DiffBp a
   if (!is_node(a, x, y))
     return;
   const size_t c = (size_t)cell;
-  float b[NV];
+  R b[NV];
 #pragma unroll
   for (int k = 0; k < NV; ++k)
   {
     const int d = lane + 32 * k;
-    float v = FLT_MAX;
+    R v = M::big();
     if (d < D)
     {
       v = a.data[c * D + d];
@@ -134,23 +150,24 @@ __global__ void __launch_bounds__(kDiffWarps * 32) k_soft_readout(const DiffBp a
     }
     b[k] = v;
   }
-  float lmin = FLT_MAX;
+  R lmin = M::big();
 #pragma unroll
   for (int k = 0; k < NV; ++k)
-    lmin = fminf(lmin, b[k]);
-  const float bmin = warp_min_f(lmin);
-  float e[NV], z = 0.0f, s = 0.0f;
+    lmin = M::min(lmin, b[k]);
+  const R bmin = warp_min<R>(lmin);
+  const R tau = (R)a.tau;
+  R e[NV], z = 0, s = 0;
 #pragma unroll
   for (int k = 0; k < NV; ++k)
   {
     const int d = lane + 32 * k;
-    e[k] = d < D ? expf(-(b[k] - bmin) / a.tau) : 0.0f;
+    e[k] = d < D ? M::exp(-(b[k] - bmin) / tau) : (R)0;
     z += e[k];
-    s += e[k] * (float)d;
+    s += e[k] * (R)d;
   }
-  z = warp_sum_f(z);
-  s = warp_sum_f(s);
-  const float disp = s / z;
+  z = warp_sum<R>(z);
+  s = warp_sum<R>(s);
+  const R disp = s / z;
   const double depth = 1.0 / (a.step * (double)disp + a.min_inv);
   const size_t px = (size_t)(y * 4) * a.W + x * 4;
   if (!backward)
@@ -164,14 +181,14 @@ __global__ void __launch_bounds__(kDiffWarps * 32) k_soft_readout(const DiffBp a
     return;
   // d depth / d disparity = -step * depth^2; d disparity / d b(d) =
   // -(1/tau) p(d) (d - disparity)
-  const float g_disp = (float)(-a.step * depth * depth * (double)g);
+  const R g_disp = (R)(-a.step * depth * depth * (double)g);
 #pragma unroll
   for (int k = 0; k < NV; ++k)
   {
     const int d = lane + 32 * k;
     if (d >= D)
       continue;
-    const float gb = g_disp * (-(e[k] / z) * ((float)d - disp) / a.tau);
+    const R gb = g_disp * (-(e[k] / z) * ((R)d - disp) / tau);
     if (x != 0)
       a.A[kRight][(c - 1) * D + d] += gb;
     if (x != w - 1)
@@ -184,9 +201,10 @@ __global__ void __launch_bounds__(kDiffWarps * 32) k_soft_readout(const DiffBp a
 }
 
 // ------------------------------------------------------------ BP adjoint
-template <int D>
-__global__ void __launch_bounds__(kDiffWarps * 32) k_bp_sweep_bwd(const DiffBp a)
+template <int D, class R>
+__global__ void __launch_bounds__(kDiffWarps * 32) k_bp_sweep_bwd(const DiffBpR<R> a)
 {
+  using M = Real<R>;
   constexpr int NV = (D + 31) / 32;
   const int lane = threadIdx.x & 31;
   const int w = a.w, h = a.h, hw = (w + 1) / 2;
@@ -199,31 +217,31 @@ __global__ void __launch_bounds__(kDiffWarps * 32) k_bp_sweep_bwd(const DiffBp a
     return;
   const bool has_u = y > 0, has_d = y < h - 1, has_l = x > 0, has_r = x < w - 1;
   const size_t c = (size_t)y * w + x;
-  float dat[NV], fu[NV], fd[NV], fl[NV], fr[NV];
-  float gu[NV], gd[NV], gl[NV], gr[NV];
+  R dat[NV], fu[NV], fd[NV], fl[NV], fr[NV];
+  R gu[NV], gd[NV], gl[NV], gr[NV];
 #pragma unroll
   for (int k = 0; k < NV; ++k)
   {
     const int d = lane + 32 * k;
     const bool in = d < D;
-    dat[k] = in ? a.data[c * D + d] : 0.0f;
-    fu[k] = (in && has_u) ? a.S[kDown][(c - w) * D + d] : 0.0f;
-    fd[k] = (in && has_d) ? a.S[kUp][(c + w) * D + d] : 0.0f;
-    fl[k] = (in && has_l) ? a.S[kRight][(c - 1) * D + d] : 0.0f;
-    fr[k] = (in && has_r) ? a.S[kLeft][(c + 1) * D + d] : 0.0f;
-    gu[k] = gd[k] = gl[k] = gr[k] = 0.0f;
+    dat[k] = in ? a.data[c * D + d] : (R)0;
+    fu[k] = (in && has_u) ? a.S[kDown][(c - w) * D + d] : (R)0;
+    fd[k] = (in && has_d) ? a.S[kUp][(c + w) * D + d] : (R)0;
+    fl[k] = (in && has_l) ? a.S[kRight][(c - 1) * D + d] : (R)0;
+    fr[k] = (in && has_r) ? a.S[kLeft][(c + 1) * D + d] : (R)0;
+    gu[k] = gd[k] = gl[k] = gr[k] = (R)0;
   }
-  const float P1 = a.P1, P2 = a.P2;
-  float gp1 = 0.0f, gp2 = 0.0f;
+  const R P1 = (R)a.P1, P2 = (R)a.P2;
+  R gp1 = 0, gp2 = 0;
 #pragma unroll
   for (int dir = 0; dir < 4; ++dir)
   {
-    float hv[NV];
-    float lmin = FLT_MAX;
+    R hv[NV];
+    R lmin = M::big();
 #pragma unroll
     for (int k = 0; k < NV; ++k)
     {
-      float v = dat[k];
+      R v = dat[k];
       if (dir != kUp && has_u)
         v += fu[k];
       if (dir != kDown && has_d)
@@ -232,10 +250,10 @@ __global__ void __launch_bounds__(kDiffWarps * 32) k_bp_sweep_bwd(const DiffBp a
         v += fl[k];
       if (dir != kRight && has_r)
         v += fr[k];
-      hv[k] = (lane + 32 * k < D) ? v : FLT_MAX;
-      lmin = fminf(lmin, hv[k]);
+      hv[k] = (lane + 32 * k < D) ? v : M::big();
+      lmin = M::min(lmin, hv[k]);
     }
-    const float hmin = warp_min_f(lmin);
+    const R hmin = warp_min<R>(lmin);
     // the first hypothesis attaining the minimum
     int amin = D;
 #pragma unroll
@@ -246,26 +264,26 @@ __global__ void __launch_bounds__(kDiffWarps * 32) k_bp_sweep_bwd(const DiffBp a
         amin = 32 * k + __ffs(bal) - 1;
     }
     // adjoint of the outgoing message, minus its mean
-    float gm[NV], gsum = 0.0f;
+    R gm[NV], gsum = 0;
 #pragma unroll
     for (int k = 0; k < NV; ++k)
     {
       const int d = lane + 32 * k;
-      gm[k] = d < D ? a.A[dir][c * D + d] : 0.0f;
+      gm[k] = d < D ? a.A[dir][c * D + d] : (R)0;
       gsum += gm[k];
     }
-    const float gmean = warp_sum_f(gsum) / (float)D;
+    const R gmean = warp_sum<R>(gsum) / (R)D;
     // selected term of every minimum: 0 own, 1 from d-1, 2 from d+1, 3 P2
     int sel[NV];
-    float own[NV], to_prev[NV], to_next[NV], s3 = 0.0f;
+    R own[NV], to_prev[NV], to_next[NV], s3 = 0;
 #pragma unroll
     for (int k = 0; k < NV; ++k)
     {
       const int d = lane + 32 * k;
-      float prev, next;
+      R prev, next;
       neighbours<NV>(hv, lane, k, prev, next);
-      gm[k] = d < D ? gm[k] - gmean : 0.0f;
-      float best = hv[k];
+      gm[k] = d < D ? gm[k] - gmean : (R)0;
+      R best = hv[k];
       int s = 0;
       if (d > 0 && prev + P1 < best)
       {
@@ -280,9 +298,9 @@ __global__ void __launch_bounds__(kDiffWarps * 32) k_bp_sweep_bwd(const DiffBp a
       if (hmin + P2 < best)
         s = 3;
       sel[k] = d < D ? s : 0;
-      own[k] = sel[k] == 0 ? gm[k] : 0.0f;
-      to_prev[k] = sel[k] == 1 ? gm[k] : 0.0f; // lands on h(d-1)
-      to_next[k] = sel[k] == 2 ? gm[k] : 0.0f; // lands on h(d+1)
+      own[k] = sel[k] == 0 ? gm[k] : (R)0;
+      to_prev[k] = sel[k] == 1 ? gm[k] : (R)0; // lands on h(d-1)
+      to_next[k] = sel[k] == 2 ? gm[k] : (R)0; // lands on h(d+1)
       if (sel[k] == 1 || sel[k] == 2)
         gp1 += gm[k];
       if (sel[k] == 3)
@@ -291,24 +309,24 @@ __global__ void __launch_bounds__(kDiffWarps * 32) k_bp_sweep_bwd(const DiffBp a
         s3 += gm[k];
       }
     }
-    s3 = warp_sum_f(s3);
-    float gh[NV];
+    s3 = warp_sum<R>(s3);
+    R gh[NV];
 #pragma unroll
     for (int k = 0; k < NV; ++k)
     {
       // h(d) receives to_prev from d+1 and to_next from d-1
-      float from_next, unused, from_prev;
+      R from_next, unused, from_prev;
       neighbours<NV>(to_prev, lane, k, unused, from_next);
       neighbours<NV>(to_next, lane, k, from_prev, unused);
       const int d = lane + 32 * k;
-      float v = own[k];
+      R v = own[k];
       if (d + 1 < D)
         v += from_next;
       if (d > 0)
         v += from_prev;
       if (d == amin)
         v += s3;
-      gh[k] = d < D ? v : 0.0f;
+      gh[k] = d < D ? v : (R)0;
     }
 #pragma unroll
     for (int k = 0; k < NV; ++k)
@@ -339,9 +357,9 @@ __global__ void __launch_bounds__(kDiffWarps * 32) k_bp_sweep_bwd(const DiffBp a
       a.A[kLeft][(c + 1) * D + d] += gr[k];
 #pragma unroll
     for (int dir = 0; dir < 4; ++dir)
-      a.A[dir][c * D + d] = 0.0f;
+      a.A[dir][c * D + d] = (R)0;
   }
-  const double t1 = warp_sum_d((double)gp1), t2 = warp_sum_d((double)gp2);
+  const double t1 = warp_sum<double>((double)gp1), t2 = warp_sum<double>((double)gp2);
   if (lane == 0)
   {
     atomicAdd(a.gP, t1);
@@ -351,9 +369,10 @@ __global__ void __launch_bounds__(kDiffWarps * 32) k_bp_sweep_bwd(const DiffBp a
 
 // adjoint of the copy-down: every parent message adds the adjoints of its
 // (up to four) children's starting messages
+template <class R>
 __global__ void __launch_bounds__(256)
-    k_msg_downsample_add(const MsgPtrs child, int cw, int ch, const MsgPtrs parent, int pw, int ph,
-                         int D)
+    k_msg_downsample_add(const MsgPtrsR<R> child, int cw, int ch, const MsgPtrsR<R> parent,
+                         int pw, int ph, int D)
 {
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long)pw * ph * D)
@@ -363,7 +382,7 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
   for (int m = 0; m < 4; ++m)
   {
-    float s = 0.0f;
+    R s = 0;
     for (int j = 0; j < 2; ++j)
       for (int i = 0; i < 2; ++i)
       {
@@ -372,6 +391,129 @@ __global__ void __launch_bounds__(256)
           s += child.m[m][((size_t)y * cw + x) * D + d];
       }
     parent.m[m][(size_t)p * D + d] += s;
+  }
+}
+
+// ------------------------------------------- FP64 BP forward (gradient check)
+__global__ void __launch_bounds__(256) k_widen(const float *in, double *out, long n)
+{
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n)
+    out[t] = (double)in[t];
+}
+
+// cost_distribute (bpextract.cu:169-198) in FP64: children summed x offset
+// outer, y offset inner
+__global__ void __launch_bounds__(256)
+    k_pyramid64(const double *fine, int fw, int fh, double *coarse, int cw, int ch, int D)
+{
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)cw * ch * D)
+    return;
+  const int p = (int)(t / D), d = (int)(t - (long)p * D);
+  const int x = p % cw, y = p / cw;
+  double s = 0.0;
+  for (int i = 0; i < 2; ++i)
+    for (int j = 0; j < 2; ++j)
+      if (2 * x + i < fw && 2 * y + j < fh)
+        s += fine[((size_t)(2 * y + j) * fw + (2 * x + i)) * D + d];
+  coarse[t] = s;
+}
+
+// the reference's copy-down of the parent's messages (upsample,
+// bpextract.cu:374-395), zeros at the coarsest level (bpextract.cu:87-90)
+__global__ void __launch_bounds__(256)
+    k_msg_inherit_all64(const MsgPtrs64 parent, int has_parent, int pw, const MsgPtrs64 child,
+                        int cw, int ch, int D)
+{
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)cw * ch * D)
+    return;
+  const int p = (int)(t / D), d = (int)(t - (long)p * D);
+  const int x = p % cw, y = p / cw;
+  const size_t src = ((size_t)(y >> 1) * pw + (x >> 1)) * D + d;
+#pragma unroll
+  for (int m = 0; m < 4; ++m)
+    child.m[m][t] = has_parent ? parent.m[m][src] : 0.0;
+}
+
+// one half-sweep (bp, bpextract.cu:200-312) in FP64, a warp per cell of the
+// colour, messages M updated in place
+template <int D>
+__global__ void __launch_bounds__(kDiffWarps * 32)
+    k_bp_sweep_fwd64(const DiffBp64 a, const MsgPtrs64 M)
+{
+  using RM = Real<double>;
+  constexpr int NV = (D + 31) / 32;
+  const int lane = threadIdx.x & 31;
+  const int w = a.w, h = a.h, hw = (w + 1) / 2;
+  const int item = blockIdx.x * kDiffWarps + (threadIdx.x >> 5);
+  if (item >= hw * h)
+    return;
+  const int y = item / hw;
+  const int x = 2 * (item - y * hw) + ((y + a.parity) & 1);
+  if (x >= w || skipped(a, x, y))
+    return;
+  const bool has_u = y > 0, has_d = y < h - 1, has_l = x > 0, has_r = x < w - 1;
+  const size_t c = (size_t)y * w + x;
+  double dat[NV], fu[NV], fd[NV], fl[NV], fr[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k)
+  {
+    const int d = lane + 32 * k;
+    const bool in = d < D;
+    dat[k] = in ? a.data[c * D + d] : 0.0;
+    fu[k] = (in && has_u) ? M.m[kDown][(c - w) * D + d] : 0.0;
+    fd[k] = (in && has_d) ? M.m[kUp][(c + w) * D + d] : 0.0;
+    fl[k] = (in && has_l) ? M.m[kRight][(c - 1) * D + d] : 0.0;
+    fr[k] = (in && has_r) ? M.m[kLeft][(c + 1) * D + d] : 0.0;
+  }
+  const double P1 = a.P1, P2 = a.P2;
+#pragma unroll
+  for (int dir = 0; dir < 4; ++dir)
+  {
+    double hv[NV];
+    double lmin = RM::big();
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+    {
+      double v = dat[k];
+      if (dir != kUp && has_u)
+        v += fu[k];
+      if (dir != kDown && has_d)
+        v += fd[k];
+      if (dir != kLeft && has_l)
+        v += fl[k];
+      if (dir != kRight && has_r)
+        v += fr[k];
+      hv[k] = (lane + 32 * k < D) ? v : RM::big();
+      lmin = fmin(lmin, hv[k]);
+    }
+    const double hmin = warp_min<double>(lmin);
+    double m[NV], msum = 0.0;
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+    {
+      const int d = lane + 32 * k;
+      double prev, next;
+      neighbours<NV>(hv, lane, k, prev, next);
+      double v = hv[k];
+      if (d > 0)
+        v = fmin(v, prev + P1);
+      if (d < D - 1)
+        v = fmin(v, next + P1);
+      m[k] = fmin(v, hmin + P2);
+      if (d < D)
+        msum += m[k];
+    }
+    const double mean = warp_sum<double>(msum) / (double)D;
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+    {
+      const int d = lane + 32 * k;
+      if (d < D)
+        M.m[dir][c * D + d] = m[k] - mean;
+    }
   }
 }
 
@@ -593,19 +735,19 @@ __global__ void __launch_bounds__(256) k_fuse_bwd(DiffFuse f)
   f.g_depth[idx] = ratio > 0.60 ? (float)(mu_p.g * (double)f.g_fused[idx]) : 0.0f;
 }
 
-template <int D>
-void readout_d(const DiffBp &a, int backward, cudaStream_t s)
+template <int D, class R>
+void readout_d(const DiffBpR<R> &a, int backward, cudaStream_t s)
 {
   const int cells = a.w * a.h;
-  k_soft_readout<D><<<(cells + kDiffWarps - 1) / kDiffWarps, kDiffWarps * 32, 0, s>>>(a,
-                                                                                     backward);
+  k_soft_readout<D, R><<<(cells + kDiffWarps - 1) / kDiffWarps, kDiffWarps * 32, 0, s>>>(
+      a, backward);
 }
 
-template <int D>
-void bwd_d(const DiffBp &a, cudaStream_t s)
+template <int D, class R>
+void bwd_d(const DiffBpR<R> &a, cudaStream_t s)
 {
   const int items = ((a.w + 1) / 2) * a.h;
-  k_bp_sweep_bwd<D><<<(items + kDiffWarps - 1) / kDiffWarps, kDiffWarps * 32, 0, s>>>(a);
+  k_bp_sweep_bwd<D, R><<<(items + kDiffWarps - 1) / kDiffWarps, kDiffWarps * 32, 0, s>>>(a);
 }
 
 template <class F>
@@ -629,18 +771,77 @@ void launch_soft_readout(const DiffBp &a, int backward, cudaStream_t s)
   by_d(a.D, [&](auto dc) { readout_d<decltype(dc)::value>(a, backward, s); });
 }
 
+void launch_soft_readout(const DiffBp64 &a, int backward, cudaStream_t s)
+{
+  by_d(a.D, [&](auto dc) { readout_d<decltype(dc)::value>(a, backward, s); });
+}
+
 void launch_bp_sweep_bwd(const DiffBp &a, cudaStream_t s)
 {
   by_d(a.D, [&](auto dc) { bwd_d<decltype(dc)::value>(a, s); });
 }
 
-void launch_msg_downsample_add(const MsgPtrs &child, int cw, int ch, const MsgPtrs &parent,
-                               int pw, int ph, int D, cudaStream_t s)
+void launch_bp_sweep_bwd(const DiffBp64 &a, cudaStream_t s)
+{
+  by_d(a.D, [&](auto dc) { bwd_d<decltype(dc)::value>(a, s); });
+}
+
+namespace
+{
+template <class R>
+void downsample_add(const MsgPtrsR<R> &child, int cw, int ch, const MsgPtrsR<R> &parent, int pw,
+                    int ph, int D, cudaStream_t s)
 {
   const long n = (long)pw * ph * D;
   if (n > 0)
-    k_msg_downsample_add<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(child, cw, ch, parent, pw,
-                                                                     ph, D);
+    k_msg_downsample_add<R><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(child, cw, ch, parent,
+                                                                        pw, ph, D);
+}
+} // namespace
+
+void launch_msg_downsample_add(const MsgPtrs &child, int cw, int ch, const MsgPtrs &parent,
+                               int pw, int ph, int D, cudaStream_t s)
+{
+  downsample_add(child, cw, ch, parent, pw, ph, D, s);
+}
+
+void launch_msg_downsample_add(const MsgPtrs64 &child, int cw, int ch, const MsgPtrs64 &parent,
+                               int pw, int ph, int D, cudaStream_t s)
+{
+  downsample_add(child, cw, ch, parent, pw, ph, D, s);
+}
+
+void launch_widen(const float *in, double *out, long n, cudaStream_t s)
+{
+  if (n > 0)
+    k_widen<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(in, out, n);
+}
+
+void launch_pyramid64(const double *fine, int fw, int fh, double *coarse, int cw, int ch, int D,
+                      cudaStream_t s)
+{
+  const long n = (long)cw * ch * D;
+  if (n > 0)
+    k_pyramid64<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(fine, fw, fh, coarse, cw, ch, D);
+}
+
+void launch_msg_inherit_all64(const MsgPtrs64 *parent, int pw, const MsgPtrs64 &child, int cw,
+                              int ch, int D, cudaStream_t s)
+{
+  const long n = (long)cw * ch * D;
+  MsgPtrs64 none{};
+  if (n > 0)
+    k_msg_inherit_all64<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(
+        parent ? *parent : none, parent ? 1 : 0, pw, child, cw, ch, D);
+}
+
+void launch_bp_sweep_fwd64(const DiffBp64 &a, const MsgPtrs64 &M, cudaStream_t s)
+{
+  const int items = ((a.w + 1) / 2) * a.h;
+  by_d(a.D, [&](auto dc) {
+    k_bp_sweep_fwd64<decltype(dc)::value>
+        <<<(items + kDiffWarps - 1) / kDiffWarps, kDiffWarps * 32, 0, s>>>(a, M);
+  });
 }
 
 void launch_upw_forward(const DiffUp &u, cudaStream_t s)

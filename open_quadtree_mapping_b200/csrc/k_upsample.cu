@@ -45,38 +45,76 @@ namespace qm
 namespace
 {
 
-// per line: w (weights, then alpha), rd / ri (right-hand sides, then the
-// scaled right-hand sides, the forward values and the solution), cp (pivots)
-constexpr int kArrays = 4;
+// Dynamic shared memory of both solvers, addressed by byte offsets from this
+// one symbol so that every access is a shared-memory access.  Block layout:
+// the 256-entry weight table, then one line after the other.
+extern __shared__ __align__(16) unsigned char g_smem[];
+
+constexpr int kTableBytes = 256 * sizeof(float);
+
+__device__ __forceinline__ float *smf(int byte_off)
+{
+  return reinterpret_cast<float *>(g_smem + byte_off);
+}
 
 __host__ __device__ __forceinline__ int seg_len(int n) { return (n + 31) / 32; }
+// float pitch of a lane's segment (odd: lane-parallel accesses hit 32
+// different banks)
 __host__ __device__ __forceinline__ int seg_pitch(int n) { return seg_len(n) | 1; }
-// floats of one array of a line of n samples (+1 for the closing weight)
-__host__ __device__ __forceinline__ int line_floats(int n) { return 32 * seg_pitch(n) + 1; }
-
-struct LineBuf
+// byte pitch of a lane's segment of image bytes: 4 x odd, so that the 32
+// lanes' bytes at the same step lie in 32 different bank words
+__host__ __device__ __forceinline__ int seg_bytes(int n) { return (((seg_len(n) + 3) / 4) | 1) * 4; }
+__host__ __device__ __forceinline__ int farray_bytes(int n)
 {
-  float *w, *rd, *ri, *cp;
-  int n, m, mp;
-  __device__ __forceinline__ int pos(int k) const
+  return (32 * seg_pitch(n) * (int)sizeof(float) + 15) & ~15;
+}
+// bytes of one line: three float arrays (right-hand sides, pivots) and the
+// image bytes
+__host__ __device__ __forceinline__ int line_bytes(int n)
+{
+  return 3 * farray_bytes(n) + ((32 * seg_bytes(n) + 15) & ~15);
+}
+
+// One line of n samples in shared memory, as byte offsets: rd / ri hold the
+// two right-hand sides (the sparse depth and its indicator), later their
+// forward values and the solution; cp the reciprocal pivots, later the
+// eliminated super-diagonal; img the line's image bytes, from which every
+// pass looks the weights up again.
+struct Line
+{
+  int rd, ri, cp, img;
+  int n, m, mp, bp;
+  float w_close; // weight between samples n - 1 and n (the closing weight)
+  __device__ __forceinline__ int fpos(int k) const
   {
     const int l = k / m;
     return l * mp + (k - l * m);
   }
+  __device__ __forceinline__ int bpos(int k) const
+  {
+    const int l = k / m;
+    return l * bp + (k - l * m);
+  }
+  __device__ __forceinline__ float &RD(int p) const { return smf(rd)[p]; }
+  __device__ __forceinline__ float &RI(int p) const { return smf(ri)[p]; }
+  __device__ __forceinline__ float &CP(int p) const { return smf(cp)[p]; }
+  __device__ __forceinline__ int I(int k) const { return g_smem[img + bpos(k)]; }
 };
 
-__device__ __forceinline__ LineBuf line_buf(float *base, int n)
+__device__ __forceinline__ Line line_at(int base, int n, float w_close)
 {
-  LineBuf b;
-  const int L = line_floats(n);
-  b.w = base;
-  b.rd = base + L;
-  b.ri = base + 2 * L;
-  b.cp = base + 3 * L;
-  b.n = n;
-  b.m = seg_len(n);
-  b.mp = seg_pitch(n);
-  return b;
+  Line L;
+  const int fb = farray_bytes(n);
+  L.rd = base;
+  L.ri = base + fb;
+  L.cp = base + 2 * fb;
+  L.img = base + 3 * fb;
+  L.n = n;
+  L.m = seg_len(n);
+  L.mp = seg_pitch(n);
+  L.bp = seg_bytes(n);
+  L.w_close = w_close;
+  return L;
 }
 
 // weight between neighbours with intensities a (current) and b (previous),
@@ -86,6 +124,23 @@ __device__ __forceinline__ float edge_weight(float a, float b, double sigma)
 {
   const float diff = a - b;
   return A::exp((float)((double)(-diff * diff) / sigma));
+}
+
+// The weight depends only on |I_k - I_{k-1}| (integers 0..255): a block
+// tabulates edge_weight for every difference once and the passes look it
+// up (the same values the expression gives pixel by pixel).
+template <class A>
+__device__ __forceinline__ void build_weight_table(double sigma)
+{
+  for (int t = threadIdx.x; t < 256; t += blockDim.x)
+    smf(0)[t] = edge_weight<A>((float)t, 0.0f, sigma);
+}
+
+// weight between samples k - 1 and k of the line (k in 1 .. n - 1), given
+// their intensities
+__device__ __forceinline__ float table_weight(int a, int b)
+{
+  return smf(0)[a > b ? a - b : b - a];
 }
 
 struct Mat2
@@ -122,31 +177,51 @@ struct Aff
   float g, hd, hi; // z -> g z + h (two right-hand sides)
 };
 
-// Solves the line held in `b` (w, rd, ri filled) and leaves the solution in
-// rd (depth) and ri (indicator).  Whole warp.  Every element is rewritten in
-// place by the lane that owns it, except w[e] (the first weight of the next
-// segment), which each lane reads before the pass that overwrites w.
-__device__ void solve_line(const LineBuf &b, double lam)
+// Walks the weights of segment [s, e): calls f(k, wl, wr) with the weights
+// to the left and right of sample k.  w_0 = 0, w_n = the closing weight,
+// every other from the table.
+template <class Fn>
+__device__ __forceinline__ void walk_weights(const Line &L, int s, int e, Fn &&f)
+{
+  if (s >= e)
+    return;
+  int Ik = L.I(s);
+  float wl = s == 0 ? 0.0f : table_weight(Ik, L.I(s - 1));
+  for (int k = s; k < e; ++k)
+  {
+    float wr;
+    int In = 0;
+    if (k + 1 < L.n)
+    {
+      In = L.I(k + 1);
+      wr = table_weight(In, Ik);
+    }
+    else
+      wr = L.w_close;
+    f(k, wl, wr);
+    wl = wr;
+    Ik = In;
+  }
+}
+
+// Solves the line (rd, ri and img filled) and leaves the solution in rd
+// (depth) and ri (indicator).  Whole warp; every float element is rewritten
+// in place by the lane that owns it (the image bytes are read-only).
+__device__ __forceinline__ void solve_line(const Line &L, double lam)
 {
   const int lane = threadIdx.x & 31;
-  const int s = min(lane * b.m, b.n);
-  const int e = min(s + b.m, b.n);
-  const int base = lane * b.mp; // smem position of element s
-  // right weight of the segment's last element
-  const float w_end = b.w[e < b.n ? b.pos(e) : 32 * b.mp];
-  __syncwarp();
+  const int s = min(lane * L.m, L.n);
+  const int e = min(s + L.m, L.n);
+  const int base = lane * L.mp; // float position of element s
   // -------- pivots: segment Moebius product (apply element s first).  The
   // entries grow by at most 1 + 2*lambda per element, far inside the double
   // range for segments of <= 128 elements, so no per-step rescaling.
   Mat2 P{1.0, 0.0, 0.0, 1.0};
-  for (int k = s; k < e; ++k)
-  {
-    const int p = base + (k - s);
-    const double wl = b.w[p];
-    const double wr = k + 1 < e ? b.w[p + 1] : w_end;
+  walk_weights(L, s, e, [&](int, float wl_f, float wr_f) {
+    const double wl = wl_f, wr = wr_f;
     const double a = -lam * wl, bb = 1.0 + lam * (wl + wr), c = -lam * wr;
     P = Mat2{c * P.c, c * P.d, bb * P.c - a * P.a, bb * P.d - a * P.b};
-  }
+  });
   P = renorm(P);
   // inclusive scan (later segments on the left), then exclusive
 #pragma unroll
@@ -160,35 +235,27 @@ __device__ void solve_line(const LineBuf &b, double lam)
   if (lane == 0)
     E = Mat2{1.0, 0.0, 0.0, 1.0};
   const double z0 = E.b / E.d; // incoming pivot c'_{s-1} (0 for lane 0)
-  // -------- pivots of the segment (FP64), forward RHS composition (FP32).
-  // With the running product Q of the segment's Moebius maps, c'_k =
-  // (Q.a z0 + Q.b) / D_k where D_k = Q.c z0 + Q.d, and den_k = D_k / D_{k-1},
-  // so 1/den_k = D_{k-1} / D_k and c'_k = c_k / den_k.  Only the 2x2 products
-  // form the serial chain; the one division per element does not feed back.
-  // The forward recurrence d'_k = alpha_k d'_{k-1} + r_k / den_k keeps
-  // alpha_k = -a_k / den_k (in w) and r_k / den_k (in rd, ri).
+  // -------- reciprocal pivots of the segment (FP64), forward RHS
+  // composition (FP32).  With the running product Q of the segment's Moebius
+  // maps, D_k = Q.c z0 + Q.d and den_k = D_k / D_{k-1}, so 1/den_k =
+  // D_{k-1} / D_k: only the 2x2 products form the serial chain.  The forward
+  // recurrence d'_k = alpha_k d'_{k-1} + r_k / den_k has alpha_k = -a_k /
+  // den_k; 1/den_k is kept (as float) for the next pass.
   Mat2 Q{1.0, 0.0, 0.0, 1.0};
   double Dprev = 1.0;
   Aff F{1.0f, 0.0f, 0.0f};
-  for (int k = s; k < e; ++k)
-  {
+  walk_weights(L, s, e, [&](int k, float wl_f, float wr_f) {
     const int p = base + (k - s);
-    const double wl = b.w[p];
-    const double wr = k + 1 < e ? b.w[p + 1] : w_end;
+    const double wl = wl_f, wr = wr_f;
     const double a = -lam * wl, bb = 1.0 + lam * (wl + wr), c = -lam * wr;
     Q = Mat2{c * Q.c, c * Q.d, bb * Q.c - a * Q.a, bb * Q.d - a * Q.b};
     const double Dk = Q.c * z0 + Q.d;
-    const double inv = Dprev / Dk; // 1 / den_k
+    const float invf = (float)(Dprev / Dk);
     Dprev = Dk;
-    b.cp[p] = (float)(c * inv);
-    const float invf = (float)inv;
+    L.CP(p) = invf;
     const float alpha = (float)(lam * wl) * invf;
-    const float qd = b.rd[p] * invf, qi = b.ri[p] * invf;
-    b.w[p] = alpha;
-    b.rd[p] = qd;
-    b.ri[p] = qi;
-    F = Aff{alpha * F.g, alpha * F.hd + qd, alpha * F.hi + qi};
-  }
+    F = Aff{alpha * F.g, alpha * F.hd + L.RD(p) * invf, alpha * F.hi + L.RI(p) * invf};
+  });
 #pragma unroll
   for (int off = 1; off < 32; off <<= 1)
   {
@@ -202,19 +269,21 @@ __device__ void solve_line(const LineBuf &b, double lam)
   float iprev = __shfl_up_sync(0xffffffffu, F.hi, 1);
   if (lane == 0)
     dprev = iprev = 0.0f;
-  // -------- forward RHS of the segment, back-substitution composition
+  // -------- forward values of the segment, eliminated super-diagonal
+  // c'_k = c_k / den_k, back-substitution composition
   Aff G{1.0f, 0.0f, 0.0f};
-  for (int k = s; k < e; ++k)
-  {
+  walk_weights(L, s, e, [&](int k, float wl_f, float wr_f) {
     const int p = base + (k - s);
-    const float alpha = b.w[p];
-    dprev = alpha * dprev + b.rd[p];
-    iprev = alpha * iprev + b.ri[p];
-    b.rd[p] = dprev;
-    b.ri[p] = iprev;
-    const float cpk = b.cp[p];
+    const float invf = L.CP(p);
+    const float alpha = (float)(lam * (double)wl_f) * invf;
+    const float cpk = (float)(-lam * (double)wr_f * (double)invf);
+    dprev = alpha * dprev + L.RD(p) * invf;
+    iprev = alpha * iprev + L.RI(p) * invf;
+    L.RD(p) = dprev;
+    L.RI(p) = iprev;
+    L.CP(p) = cpk;
     G = Aff{-G.g * cpk, G.g * dprev + G.hd, G.g * iprev + G.hi};
-  }
+  });
   // suffix scan: lane l composes with the segments after it
 #pragma unroll
   for (int off = 1; off < 32; off <<= 1)
@@ -233,11 +302,11 @@ __device__ void solve_line(const LineBuf &b, double lam)
   for (int k = e - 1; k >= s; --k)
   {
     const int p = base + (k - s);
-    const float cpk = b.cp[p];
-    zd = b.rd[p] - cpk * zd;
-    zi = b.ri[p] - cpk * zi;
-    b.rd[p] = zd;
-    b.ri[p] = zi;
+    const float cpk = L.CP(p);
+    zd = L.RD(p) - cpk * zd;
+    zi = L.RI(p) - cpk * zi;
+    L.RD(p) = zd;
+    L.RI(p) = zi;
   }
   __syncwarp();
 }
@@ -246,17 +315,20 @@ template <class A>
 __global__ void __launch_bounds__(kMaxRowWarps * 32)
     k_row_solve(const __grid_constant__ Batch B, KParams kp, int max_n)
 {
-  extern __shared__ float smem[];
   int lb;
   const JobDesc &J = job_of(B, lb);
+  build_weight_table<A>(kp.up_sigma);
+  __syncthreads();
   const int W = J.W, H = J.H;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int y = lb * (int)(blockDim.x >> 5) + warp;
   if (y >= H)
     return;
   const int n = W / 16 * 16;
-  LineBuf b = line_buf(smem + warp * kArrays * line_floats(max_n), n);
   const uint8_t *img = J.ref + (size_t)y * J.ref_pitch;
+  const float w_close = (n < W) ? edge_weight<A>((float)img[n], (float)img[n - 1], kp.up_sigma)
+                                : (W % 16 != 0 ? 1.0f : 0.0f);
+  const Line L = line_at(kTableBytes + warp * line_bytes(max_n), n, w_close);
   const float *sp = J.sparse + (size_t)y * W;
   // the row's fusion z-buffer keys start empty for this frame's fusion (the
   // previous frame's update left them set); coalesced stores in a
@@ -264,25 +336,21 @@ __global__ void __launch_bounds__(kMaxRowWarps * 32)
   unsigned long long *zk = J.zkey ? J.zkey + (size_t)y * W : nullptr;
   for (int k = lane; k < n; k += 32)
   {
-    const int p = b.pos(k);
+    const int p = L.fpos(k);
     if (zk)
       zk[k] = ~0ull;
-    const float I = (float)img[k];
-    b.w[p] = k == 0 ? 0.0f : edge_weight<A>(I, (float)img[k - 1], kp.up_sigma);
+    g_smem[L.img + L.bpos(k)] = img[k];
     const float d = sp[k];
-    b.rd[p] = d;
-    b.ri[p] = d > 0.0f ? 1.0f : 0.0f;
+    L.RD(p) = d;
+    L.RI(p) = d > 0.0f ? 1.0f : 0.0f;
   }
-  if (lane == 0)
-    b.w[32 * b.mp] = (n < W) ? edge_weight<A>((float)img[n], (float)img[n - 1], kp.up_sigma)
-                             : (W % 16 != 0 ? 1.0f : 0.0f);
   __syncwarp();
-  solve_line(b, kp.up_lambda);
+  solve_line(L, kp.up_lambda);
   float2 *out = J.rowres + (size_t)y * W;
   for (int k = lane; k < n; k += 32)
   {
-    const int p = b.pos(k);
-    out[k] = make_float2(b.rd[p], b.ri[p]);
+    const int p = L.fpos(k);
+    out[k] = make_float2(L.RD(p), L.RI(p));
   }
 }
 
@@ -290,15 +358,15 @@ template <class A>
 __global__ void __launch_bounds__(kMaxColLines * 32)
     k_col_solve(const __grid_constant__ Batch B, KParams kp, int max_n)
 {
-  extern __shared__ float smem[];
   int lb;
   const JobDesc &J = job_of(B, lb);
+  build_weight_table<A>(kp.up_sigma);
   const int W = J.W, H = J.H;
   const int warp = threadIdx.x >> 5;
   const int lines = blockDim.x >> 5;
   const int x0 = lb * lines;
   const int n = H / 8 * 8;
-  const int per_line = kArrays * line_floats(max_n);
+  const int per_line = line_bytes(max_n);
   // cooperative stripe load: row k, column x0 + c
   for (int t = threadIdx.x; t < n * lines; t += blockDim.x)
   {
@@ -306,33 +374,33 @@ __global__ void __launch_bounds__(kMaxColLines * 32)
     const int x = x0 + c;
     if (x >= W)
       continue;
-    LineBuf b = line_buf(smem + c * per_line, n);
-    const int p = b.pos(k);
+    const Line L = line_at(kTableBytes + c * per_line, n, 0.0f);
+    const int p = L.fpos(k);
     const float2 r = J.rowres[(size_t)k * W + x];
-    b.rd[p] = r.x;
-    b.ri[p] = r.y;
-    const float I = (float)J.ref[(size_t)k * J.ref_pitch + x];
-    b.w[p] = k == 0 ? 0.0f
-                    : edge_weight<A>(I, (float)J.ref[(size_t)(k - 1) * J.ref_pitch + x],
-                                     kp.up_sigma);
-    if (k == n - 1)
-      b.w[32 * b.mp] =
-          (n < H) ? edge_weight<A>((float)J.ref[(size_t)n * J.ref_pitch + x], I, kp.up_sigma)
-                  : (H % 16 != 0 ? 1.0f : 0.0f);
+    L.RD(p) = r.x;
+    L.RI(p) = r.y;
+    g_smem[L.img + L.bpos(k)] = J.ref[(size_t)k * J.ref_pitch + x];
   }
   __syncthreads();
-  if (x0 + warp < W)
-    solve_line(line_buf(smem + warp * per_line, n), kp.up_lambda);
+  const int x = x0 + warp;
+  if (x < W)
+  {
+    const float w_close =
+        (n < H) ? edge_weight<A>((float)J.ref[(size_t)n * J.ref_pitch + x],
+                                 (float)J.ref[(size_t)(n - 1) * J.ref_pitch + x], kp.up_sigma)
+                : (H % 16 != 0 ? 1.0f : 0.0f);
+    solve_line(line_at(kTableBytes + warp * per_line, n, w_close), kp.up_lambda);
+  }
   __syncthreads();
   for (int t = threadIdx.x; t < n * lines; t += blockDim.x)
   {
     const int k = t / lines, c = t - k * lines;
-    const int x = x0 + c;
-    if (x >= W)
+    const int xc = x0 + c;
+    if (xc >= W)
       continue;
-    LineBuf b = line_buf(smem + c * per_line, n);
-    const int p = b.pos(k);
-    J.dense[(size_t)k * W + x] = A::div(b.rd[p], b.ri[p]);
+    const Line L = line_at(kTableBytes + c * per_line, n, 0.0f);
+    const int p = L.fpos(k);
+    J.dense[(size_t)k * W + xc] = A::div(L.RD(p), L.RI(p));
   }
 }
 
@@ -340,11 +408,11 @@ __global__ void __launch_bounds__(kMaxColLines * 32)
 
 size_t row_solve_smem(int max_w, int rows)
 {
-  return sizeof(float) * rows * kArrays * line_floats(max_w);
+  return (size_t)kTableBytes + (size_t)rows * line_bytes(max_w);
 }
 size_t col_solve_smem(int max_h, int lines)
 {
-  return sizeof(float) * lines * kArrays * line_floats(max_h);
+  return (size_t)kTableBytes + (size_t)lines * line_bytes(max_h);
 }
 
 void prepare_upsample_kernels()

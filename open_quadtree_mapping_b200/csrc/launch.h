@@ -69,6 +69,19 @@ void launch_bp_sweep(const Batch &B, int blocks, int d, int level, int it, KPara
 // level's own buffers (all cells' starting messages already written)
 void launch_bp_sweep_own(const Batch &B, int blocks, int d, int level, int parity, KParams kp,
                          int arith, cudaStream_t s, int warps = kCellWarps);
+// Coarse BP levels in one launch (k_bp_coarse): levels hi down to lo, every
+// one with at least two half-sweeps (their first two write the inherited
+// messages), one cluster of kCoarseCtas blocks of kCoarseThreads threads per
+// job, jobs j0 .. j0 + jobs - 1 of the batch (B.jobs null: the inline job).
+constexpr int kCoarseCtas = 8;
+constexpr int kCoarseThreads = 512;
+struct CoarsePlan
+{
+  int lo, hi;
+  int iters[kMaxLevels];
+};
+void launch_bp_coarse(const Batch &B, int j0, int jobs, int d, const CoarsePlan &plan,
+                      KParams kp, int arith, cudaStream_t s);
 void launch_extract(const Batch &B, int blocks, int d, int arith, cudaStream_t s,
                     int warps = kCellWarps);
 void launch_row_solve(const Batch &B, int blocks, KParams kp, int arith, int max_w,
@@ -94,16 +107,19 @@ void launch_point_cloud(const float *depth, size_t stride, const uint8_t *ref, s
 // ---------------------------------------------------------------------------
 // Differentiable path (k_diff.cu).
 
-// One BP level of one keyframe for the soft readout and the BP adjoint.
-struct DiffBp
+// One BP level of one keyframe for the soft readout and the BP adjoint, with
+// messages, adjoints and data terms of real type R: float for the
+// differentiable product path, double for the gradient-check mode.
+template <class R>
+struct DiffBpR
 {
   int W, H, D;           // image and hypotheses
   int w, h;              // cells of this level
   int level, parity, qt_max;
   const uint8_t *levels; // quadtree level map
-  const float *data;     // data term of this level
-  const float *S[4];     // messages read (a state snapshot, or the finals)
-  float *A[4];           // adjoint of the messages, by direction
+  const R *data;         // data term of this level
+  const R *S[4];         // messages read (a state snapshot, or the finals)
+  R *A[4];               // adjoint of the messages, by direction
   float P1, P2;
   double *gP;            // dL/dP1, dL/dP2 (accumulated)
   float tau;             // readout temperature
@@ -111,20 +127,41 @@ struct DiffBp
   float *sparse;         // readout output (W x H)
   const float *g_sparse; // its adjoint
 };
+using DiffBp = DiffBpR<float>;
+using DiffBp64 = DiffBpR<double>;
+template <class R>
+struct MsgPtrsR
+{
+  R *m[4];
+};
+using MsgPtrs = MsgPtrsR<float>;
+using MsgPtrs64 = MsgPtrsR<double>;
 // soft readout at level-0 node cells: forward writes sparse; backward adds
 // the belief adjoint to A (the four incoming messages of every node cell)
 void launch_soft_readout(const DiffBp &a, int backward, cudaStream_t s);
+void launch_soft_readout(const DiffBp64 &a, int backward, cudaStream_t s);
 // adjoint of one half-sweep of colour a.parity: reads A at the updated cells
 // (then zeroes it) and adds to A at the messages they read (a.S is the state
 // the forward half-sweep read)
 void launch_bp_sweep_bwd(const DiffBp &a, cudaStream_t s);
-struct MsgPtrs
-{
-  float *m[4];
-};
+void launch_bp_sweep_bwd(const DiffBp64 &a, cudaStream_t s);
 // parent.m[k] += sum of the (up to four) children's child.m[k], k = 0..3
 void launch_msg_downsample_add(const MsgPtrs &child, int cw, int ch, const MsgPtrs &parent,
                                int pw, int ph, int D, cudaStream_t s);
+void launch_msg_downsample_add(const MsgPtrs64 &child, int cw, int ch, const MsgPtrs64 &parent,
+                               int pw, int ph, int D, cudaStream_t s);
+// FP64 BP forward of the gradient-check mode (the product's BP is FP32):
+// out[i] = in[i] widened; the pyramid of data terms (children summed x
+// offset outer, y offset inner); every cell of a level starting from its
+// parent's messages (zeros when parent is null), as the reference's
+// copy-down; one half-sweep of colour a.parity updating M in place (a.S
+// unused)
+void launch_widen(const float *in, double *out, long n, cudaStream_t s);
+void launch_pyramid64(const double *fine, int fw, int fh, double *coarse, int cw, int ch, int D,
+                      cudaStream_t s);
+void launch_msg_inherit_all64(const MsgPtrs64 *parent, int pw, const MsgPtrs64 &child, int cw,
+                              int ch, int D, cudaStream_t s);
+void launch_bp_sweep_fwd64(const DiffBp64 &a, const MsgPtrs64 &M, cudaStream_t s);
 
 // Weighted upsampling of one image (FP64 line solves).
 struct DiffUp

@@ -295,6 +295,11 @@ class BatchDepthmap:
         """L2 budget of a BP job range (0 = all streams at once)."""
         _lib.check(_lib.lib().qm_batch_set_group_bytes(self._h, int(nbytes)))
 
+    def set_coarse_bp(self, max_cells: int) -> None:
+        """Top BP levels with at most max_cells cells in one cluster launch
+        (0 = one launch per half-sweep at every level)."""
+        _lib.check(_lib.lib().qm_batch_set_coarse_bp(self._h, int(max_cells)))
+
     TUNE_FIELDS = ("sweep_warps", "extract_warps", "row_warps", "col_lines")
 
     def set_autotune(self, on: bool) -> None:

@@ -42,38 +42,43 @@ def _with_penalties(params: Params, pen: torch.Tensor) -> Params:
 
 
 class SoftBP(torch.autograd.Function):
-    """sparse = SoftBP.apply(penalties, cost, levels, params, tau).
+    """sparse = SoftBP.apply(penalties, cost, levels, params, tau, fp64=False).
 
     penalties: (2,) float64 tensor (P1, P2); cost: (H/4, W/4, D) float32 CUDA;
     levels: (H, W) uint8 CUDA quadtree levels.  Returns (H, W) float32 with
-    the soft-readout depth at (4x, 4y) of every node cell, 0 elsewhere."""
+    the soft-readout depth at (4x, 4y) of every node cell, 0 elsewhere.
+    fp64: run the BP, the readout and the adjoint in FP64 (qm_bp_soft64_*),
+    the gradient-check mode; the default FP32 path is the fitting path."""
 
     @staticmethod
-    def forward(ctx, penalties, cost, levels, params: Params, tau: float):
+    def forward(ctx, penalties, cost, levels, params: Params, tau: float, fp64: bool = False):
         H, W = levels.shape
         p = _with_penalties(params, penalties)
         pc = QmParamsC.from_params(p)
+        L = _lib.lib()
+        ws_size, fwd = ((L.qm_bp_soft64_workspace_size, L.qm_bp_soft64_forward) if fp64 else
+                        (L.qm_bp_soft_workspace_size, L.qm_bp_soft_forward))
         n = ctypes.c_size_t()
-        _lib.check(_lib.lib().qm_bp_soft_workspace_size(W, H, ctypes.byref(pc), ctypes.byref(n)))
+        _lib.check(ws_size(W, H, ctypes.byref(pc), ctypes.byref(n)))
         ws = torch.empty(n.value, dtype=torch.uint8, device=cost.device)
         sparse = torch.empty((H, W), dtype=torch.float32, device=cost.device)
-        _lib.check(_lib.lib().qm_bp_soft_forward(_ptr(cost), W, H, _ptr(levels), ctypes.byref(pc),
-                                                 ctypes.c_float(tau), _ptr(sparse), _ptr(ws),
-                                                 n.value, _stream()))
-        ctx.state = (cost, levels, p, tau, ws, penalties.dtype, penalties.device)
+        _lib.check(fwd(_ptr(cost), W, H, _ptr(levels), ctypes.byref(pc), ctypes.c_float(tau),
+                       _ptr(sparse), _ptr(ws), n.value, _stream()))
+        ctx.state = (cost, levels, p, tau, ws, penalties.dtype, penalties.device, fp64)
         return sparse
 
     @staticmethod
     def backward(ctx, g_sparse):
-        cost, levels, p, tau, ws, dtype, device = ctx.state
+        cost, levels, p, tau, ws, dtype, device, fp64 = ctx.state
         H, W = levels.shape
         g = g_sparse.contiguous().to(torch.float32)
         gp = torch.empty(2, dtype=torch.float64, device=cost.device)
         pc = QmParamsC.from_params(p)
-        _lib.check(_lib.lib().qm_bp_soft_backward(_ptr(cost), W, H, _ptr(levels),
-                                                  ctypes.byref(pc), ctypes.c_float(tau), _ptr(g),
-                                                  _ptr(gp), _ptr(ws), ws.numel(), _stream()))
-        return gp.to(device=device, dtype=dtype), None, None, None, None
+        L = _lib.lib()
+        bwd = L.qm_bp_soft64_backward if fp64 else L.qm_bp_soft_backward
+        _lib.check(bwd(_ptr(cost), W, H, _ptr(levels), ctypes.byref(pc), ctypes.c_float(tau),
+                       _ptr(g), _ptr(gp), _ptr(ws), ws.numel(), _stream()))
+        return gp.to(device=device, dtype=dtype), None, None, None, None, None
 
 
 class UpsampleW(torch.autograd.Function):
@@ -156,11 +161,13 @@ class Keyframe:
         return self
 
 
-def forward_keyframe(kf: Keyframe, penalties, omega, params: Params, tau: float = 0.05):
+def forward_keyframe(kf: Keyframe, penalties, omega, params: Params, tau: float = 0.05,
+                     fp64: bool = False):
     """Fused depth of one keyframe as a differentiable function of
-    penalties (P1, P2) and omega."""
+    penalties (P1, P2) and omega (fp64: the soft BP in its FP64
+    gradient-check mode)."""
     kf.prepare(params)
-    sparse = SoftBP.apply(penalties, kf.cost, kf.levels, params, tau)
+    sparse = SoftBP.apply(penalties, kf.cost, kf.levels, params, tau, fp64)
     dense = UpsampleW.apply(sparse, omega, kf.ref, params)
     return Fuse.apply(dense, kf.seeds, kf.T_fuse, kf.cam, params)
 

@@ -78,7 +78,9 @@ def test_facade_matches_oracle_replay(oracle_mod, gpu):
 
 def test_batch_equals_plain_and_graph_equals_eager(gpu):
     """Three streams run batched (one launch per stage, graph replay) give
-    bit-identical maps to three single-stream runs and to eager launches."""
+    bit-identical maps to three single-stream runs, to eager launches, to
+    other BP job groupings and branch counts, and with the coarse BP levels
+    swept per launch or all levels in the cluster launch."""
     from open_quadtree_mapping_b200.depthmap import BatchDepthmap
     seqs = [sequence(s, 14, W, H) for s in (2, 3, 4)]
     p = Params.for_range(64, 0.5, 50.0)
@@ -94,6 +96,12 @@ def test_batch_equals_plain_and_graph_equals_eager(gpu):
     # branches over the halves of the streams)
     branched = BatchDepthmap([_stream_kw()] * 3, params=p)
     branched.set_branches(1)
+    # the coarse BP levels one launch per half-sweep (the reference's launch
+    # sequence), and every level in the cluster launch (extraction included)
+    coarse_off = BatchDepthmap([_stream_kw()] * 3, params=p)
+    coarse_off.set_coarse_bp(0)
+    coarse_all = BatchDepthmap([_stream_kw()] * 3, params=p)
+    coarse_all.set_coarse_bp(1 << 30)
     singles = [BatchDepthmap([_stream_kw()], params=p) for _ in range(3)]
     for i in range(14):
         imgs = [s[0][i] for s in seqs]
@@ -103,6 +111,8 @@ def test_batch_equals_plain_and_graph_equals_eager(gpu):
         assert split.add_frames(imgs, poses) == hb
         assert whole.add_frames(imgs, poses) == hb
         assert branched.add_frames(imgs, poses) == hb
+        assert coarse_off.add_frames(imgs, poses) == hb
+        assert coarse_all.add_frames(imgs, poses) == hb
         hs = [singles[k].add_frames([imgs[k]], [poses[k]])[0] for k in range(3)]
         assert hb == he == hs
         if all(hb) and i > 0:
@@ -114,6 +124,9 @@ def test_batch_equals_plain_and_graph_equals_eager(gpu):
                 assert np.array_equal(a, split.get_depth(k))
                 assert np.array_equal(a, whole.get_depth(k))
                 assert np.array_equal(a, branched.get_depth(k))
+                assert np.array_equal(a, coarse_off.get_depth(k))
+                assert np.array_equal(a, coarse_all.get_depth(k))
+                assert np.array_equal(batch.get_debug(k), coarse_off.get_debug(k))
                 assert np.array_equal(a, singles[k].get_depth(0))
                 assert np.array_equal(batch.get_debug(k), singles[k].get_debug(0))
     assert batch.last_launches() > 0
