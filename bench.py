@@ -423,10 +423,17 @@ def main():
     S = args.streams
     params = Params.for_range(D, MIN_DEPTH, MAX_DEPTH)
     t0 = time.time()
-    seqs = render_streams(args.distinct, 3000 + 100 * rank)
+    seqs = render_streams(args.distinct, 3000)
     log("rank %d: rendered %d sequences in %.1f s" % (rank, len(seqs), time.time() - t0))
     desc = dict(width=W, height=H, fx=FX, fy=FY, cx=CX, cy=CY, num_hyp=D, num_slots=SLOTS)
-    batch = BatchDepthmap([desc] * S, params=params, device=local)
+    # S * world global streams placed over the ranks by estimated bytes (equal
+    # streams: round-robin, S per rank); global stream g replays sequence
+    # g % distinct
+    from open_quadtree_mapping_b200.sharding import ShardedBatch
+    shard = ShardedBatch([desc] * (S * world), rank, world, params=params, device=local)
+    batch = shard.batch
+    seq_of = [g % len(seqs) for g in shard.mine]
+    assert len(seq_of) == S
     # pinned host frames, one per (distinct sequence, frame)
     pinned = {}
     for k, (imgs, _) in enumerate(seqs):
@@ -440,8 +447,8 @@ def main():
                   for _ in range(2)]
 
     def feed(i):
-        imgs = [pinned[(s % len(seqs), i)].numpy() for s in range(S)]
-        poses = [seqs[s % len(seqs)][1][i] for s in range(S)]
+        imgs = [pinned[(seq_of[s], i)].numpy() for s in range(S)]
+        poses = [seqs[seq_of[s]][1][i] for s in range(S)]
         return batch.add_frames(imgs, poses)
 
     for i in range(WARM_FRAMES):
@@ -480,8 +487,8 @@ def main():
 
     def e2e_step(j):
         i = WARM_FRAMES + (j % CYCLE_FRAMES)
-        imgs = [pinned[(s % len(seqs), i)].numpy() for s in range(S)]
-        poses = [seqs[s % len(seqs)][1][i] for s in range(S)]
+        imgs = [pinned[(seq_of[s], i)].numpy() for s in range(S)]
+        poses = [seqs[seq_of[s]][1][i] for s in range(S)]
         has = batch.submit(imgs, poses, outs=out_np[j % 2])
         # every step must yield S depth maps: a frame the policy skipped
         # would download nothing and inflate the rate
@@ -513,7 +520,7 @@ def main():
     from open_quadtree_mapping_b200 import stages
     lv_by_seq = {k: stages.quadtree(torch.from_numpy(np.ascontiguousarray(
         seqs[k][0][WARM_FRAMES - 1])).cuda(), params).cpu().numpy() for k in range(len(seqs))}
-    levels_list = [lv_by_seq[s % len(seqs)] for s in range(S)]
+    levels_list = [lv_by_seq[seq_of[s]] for s in range(S)]
     alg = algorithmic_bytes(levels_list, params)
     peak, peak_kind = measured_hbm_peak()
     kinds = {}
@@ -588,7 +595,8 @@ def main():
         "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "streams_per_gpu": S, "global_batch": S * world,
-                   "maps_per_step": S * world, "parallelism": "streams sharded per GPU",
+                   "maps_per_step": S * world,
+                   "parallelism": "streams placed per GPU by estimated bytes (sharding.ShardedBatch)",
                    "launch_shapes": tune,
                    "l2": "inputs larger than L2: per-GPU working set %.1f GB per step"
                          % (S * 0.08)},

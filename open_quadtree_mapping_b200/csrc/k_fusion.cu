@@ -34,6 +34,42 @@ namespace
 
 constexpr unsigned long long kEmpty = ~0ull;
 
+// e^x for the pdf's exponent x = -dm^2 / (2 var): a pixel whose squared
+// distance to its prior exceeds var has been reset to its own depth (dm =
+// 0), so x lies in [-0.5, 0].  There the Taylor series of e^x to degree 14,
+// evaluated by Horner's rule, is accurate to the last bits of a double (the
+// first dropped term is below 0.5^15 / 15! < 3e-17); any other argument
+// (NaN, inf input) takes the library exp.
+__device__ __forceinline__ double exp_pdf(double x)
+{
+  if (!(x >= -0.5 && x <= 0.0))
+    return exp(x);
+  // 1 / k!, k = 14 .. 0
+  constexpr double c[15] = {1.0 / 87178291200.0, 1.0 / 6227020800.0, 1.0 / 479001600.0,
+                            1.0 / 39916800.0,    1.0 / 3628800.0,    1.0 / 362880.0,
+                            1.0 / 40320.0,       1.0 / 5040.0,       1.0 / 720.0,
+                            1.0 / 120.0,         1.0 / 24.0,         1.0 / 6.0,
+                            0.5,                 1.0,                1.0};
+  double r = c[0];
+#pragma unroll
+  for (int k = 1; k < 15; ++k)
+    r = fma(r, x, c[k]);
+  return r;
+}
+
+// 1/v for a positive normal v: the hardware's approximate FP64 reciprocal
+// refined by two Newton-Raphson steps r <- r + r (1 - v r), each of which
+// squares the relative error (about 2^-22 -> 2^-44 -> below 2^-53).
+__device__ __forceinline__ double recip_pos(double v)
+{
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(v));
+  double e = fma(-v, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-v, r, 1.0);
+  return fma(r, e, r);
+}
+
 template <class A>
 __global__ void __launch_bounds__(kFlatThreads)
     k_fuse_transform(const __grid_constant__ Batch B)
@@ -142,20 +178,24 @@ __global__ void __launch_bounds__(kFlatThreads)
   // 1/((ab+1)(ab+2)); and a' = (e - f) / (f - e/f), b' = a' (1 - f) / f
   // share the denominator f^2 - e.  The inlier ratio that gates the output
   // is the exact quotient.
+  // var >= 0.25, c1 + c2 > 0 and (ab + 1)(ab + 2) >= 2 for every seed the
+  // pipeline produces (a, b >= 0): their reciprocals take recip_pos; the
+  // inlier ratio and the Beta update keep IEEE divisions (the ratio gates
+  // the output; f^2 - e may vanish)
   const double var = unc + s2;
-  const double ivar = 1.0 / var;
+  const double ivar = recip_pos(var);
   const double new_sq = unc * s2 * ivar;
   const double new_mu = (dep * s2 + mu * unc) * ivar;
   const double dm = dep - mu;
-  const double pdf = exp(-dm * dm * (0.5 * ivar)) * rsqrt(2.0 * M_PI * var);
+  const double pdf = exp_pdf(-dm * dm * (0.5 * ivar)) * rsqrt(2.0 * M_PI * var);
   const double ab = a + b;
   const double ratio = a / ab;
   double c1 = a * pdf;
   double c2 = b * (1.0 / 50.0);
-  const double inorm = 1.0 / (c1 + c2);
+  const double inorm = recip_pos(c1 + c2);
   c1 *= inorm;
   c2 *= inorm;
-  const double i12 = 1.0 / ((ab + 1.0) * (ab + 2.0));
+  const double i12 = recip_pos((ab + 1.0) * (ab + 2.0));
   const double i1 = (ab + 2.0) * i12;
   const double f = (c1 * (a + 1.0) + c2 * a) * i1;
   const double e = (c1 * ((a + 1.0) * (a + 2.0)) + c2 * (a * (a + 1.0))) * i12;

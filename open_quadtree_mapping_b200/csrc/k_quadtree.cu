@@ -163,14 +163,31 @@ __global__ void __launch_bounds__(kQtWarps * 32)
   const int x0 = (tile % tiles_x) * 16 + 4 * a, y0 = (tile / tiles_x) * 16 + 2 * b;
   int v[2][4];
   bool in[2][4];
+  // the lane's 4 bytes of a row as one 32-bit load when the row segment is
+  // inside the image and 4-byte aligned (every batched frame: W % 16 == 0)
+  const bool wide = x0 + 3 < W && (J.ref_pitch & 3) == 0 && ((uintptr_t)J.ref & 3) == 0;
 #pragma unroll
   for (int r = 0; r < 2; ++r)
-#pragma unroll
-    for (int c = 0; c < 4; ++c)
+  {
+    const uint8_t *row = J.ref + (size_t)(y0 + r) * J.ref_pitch + x0;
+    if (wide && y0 + r < H)
     {
-      in[r][c] = x0 + c < W && y0 + r < H;
-      v[r][c] = in[r][c] ? (int)J.ref[(size_t)(y0 + r) * J.ref_pitch + x0 + c] : 0;
+      const unsigned q = *reinterpret_cast<const unsigned *>(row);
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+      {
+        in[r][c] = true;
+        v[r][c] = (int)((q >> (8 * c)) & 0xffu);
+      }
     }
+    else
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+      {
+        in[r][c] = x0 + c < W && y0 + r < H;
+        v[r][c] = in[r][c] ? (int)row[c] : 0;
+      }
+  }
   // level 1: the lane's two 2x2 blocks
   Node n1[2];
   bool ok1[2];
@@ -201,19 +218,40 @@ __global__ void __launch_bounds__(kQtWarps * 32)
   Node n4 = merge_lane(merge_lane(n3, 2), 16);
   const bool ok4 = approve(n4, 4, kp.qt_thr);
   const int upper = ok4 ? 4 : ok3 ? 3 : ok2 ? 2 : 1;
+  const bool clear = J.sparse && !J.keep_sparse; // the debug image starts empty
 #pragma unroll
   for (int r = 0; r < 2; ++r)
+  {
+    if (y0 + r >= H)
+      continue;
+    const size_t o = (size_t)(y0 + r) * W + x0;
+    // four levels as one 32-bit store and four depths as one 16-byte store
+    // when the row segment is inside the image and aligned (the level map
+    // and the sparse image are W-pitched)
+    const bool seg = x0 + 3 < W && (W & 3) == 0;
+    if (seg && ((uintptr_t)J.levels & 3) == 0 &&
+        (!clear || ((uintptr_t)J.sparse & 15) == 0))
+    {
+      unsigned q = 0;
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        q |= (unsigned)max(ok1[c >> 1] ? upper : 0, kp.qt_min) << (8 * c);
+      *reinterpret_cast<unsigned *>(J.levels + o) = q;
+      if (clear)
+        *reinterpret_cast<float4 *>(J.sparse + o) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      continue;
+    }
 #pragma unroll
     for (int c = 0; c < 4; ++c)
     {
       if (!in[r][c])
         continue;
       const int level = ok1[c >> 1] ? upper : 0;
-      const size_t o = (size_t)(y0 + r) * W + x0 + c;
-      J.levels[o] = (uint8_t)max(level, kp.qt_min);
-      if (J.sparse && !J.keep_sparse)
-        J.sparse[o] = 0.0f; // the debug image starts empty
+      J.levels[o + c] = (uint8_t)max(level, kp.qt_min);
+      if (clear)
+        J.sparse[o + c] = 0.0f;
     }
+  }
 }
 
 } // namespace

@@ -60,3 +60,58 @@ def max_over_ranks(value: float, group=None) -> float:
     t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
     return float(t.item())
+
+
+def desc_bytes(d: dict) -> float:
+    """map_bytes of a stream descriptor (width, height, num_hyp, num_slots)."""
+    return map_bytes(int(d["width"]), int(d["height"]), int(d.get("num_hyp") or 64),
+                     int(d.get("num_slots") or 5))
+
+
+class ShardedBatch:
+    """This rank's share of a global list of camera streams.
+
+    Every rank builds the same placement (assign_streams over the streams'
+    estimated bytes), owns the streams placed on it as one batch on its own
+    GPU, and is fed the global per-tick frame lists: add_frames / submit take
+    one image and pose per GLOBAL stream and pass this rank's on.  Flags and
+    depth maps are keyed by global stream index.  No data crosses ranks.
+
+    batch_factory(descs, params=..., device=...) builds the per-rank batch
+    (default: BatchDepthmap); tests pass a stand-in."""
+
+    def __init__(self, descs, rank: int, world: int, params=None, device: int = 0,
+                 batch_factory=None):
+        if not 0 <= rank < world:
+            raise ValueError("rank %d outside world %d" % (rank, world))
+        self.n = len(descs)
+        self.mine = assign_streams([desc_bytes(d) for d in descs], world)[rank]
+        if batch_factory is None:
+            from .depthmap import BatchDepthmap as batch_factory
+        self.batch = (batch_factory([descs[i] for i in self.mine], params=params, device=device)
+                      if self.mine else None)
+
+    def _pick(self, xs):
+        if len(xs) != self.n:
+            raise ValueError("expected %d per-stream entries, got %d" % (self.n, len(xs)))
+        return [xs[i] for i in self.mine]
+
+    def add_frames(self, imgs, poses) -> dict:
+        if self.batch is None:
+            return {}
+        return dict(zip(self.mine, self.batch.add_frames(self._pick(imgs), self._pick(poses))))
+
+    def submit(self, imgs, poses, outs=None) -> dict:
+        if self.batch is None:
+            return {}
+        has = self.batch.submit(self._pick(imgs), self._pick(poses),
+                                outs=self._pick(outs) if outs is not None else None)
+        return dict(zip(self.mine, has))
+
+    def get_depth(self, i):
+        return self.batch.get_depth(self.mine.index(i))
+
+    def close(self):
+        if self.batch is not None:
+            self.batch.close()
+

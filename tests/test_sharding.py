@@ -38,6 +38,23 @@ def _free_port():
     return port
 
 
+class _FakeBatch:
+    """Stands in for BatchDepthmap: records its streams and answers flags."""
+
+    def __init__(self, descs, params=None, device=0):
+        self.descs = descs
+
+    def add_frames(self, imgs, poses):
+        assert len(imgs) == len(poses) == len(self.descs)
+        return [img["stream"] % 2 == 0 for img in imgs]
+
+    def submit(self, imgs, poses, outs=None):
+        return self.add_frames(imgs, poses)
+
+    def close(self):
+        pass
+
+
 def _worker(rank, world, port, q):
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
@@ -47,9 +64,21 @@ def _worker(rank, world, port, q):
     costs = [map_bytes(752, 480, 64)] * 5 + [map_bytes(1280, 720, 64)] * 3
     mine = assign_streams(costs, world)[rank]
     slowest = max_over_ranks(10.0 + rank)
+    # the sharded driver over the uneven 16-stream layout: this rank's batch
+    # gets its placed streams' descriptors, and frames fed as global lists
+    # reach the right streams
+    from open_quadtree_mapping_b200.sharding import ShardedBatch
+    descs = ([dict(width=640, height=480, num_hyp=48, num_slots=3)] * 6 +
+             [dict(width=752, height=480, num_hyp=64, num_slots=5)] * 6 +
+             [dict(width=1280, height=720, num_hyp=96, num_slots=10)] * 4)
+    sb = ShardedBatch(descs, rank, world, batch_factory=_FakeBatch)
+    frames = [{"stream": i} for i in range(16)]
+    flags = sb.add_frames(frames, [None] * 16)
+    sub = sb.submit(frames, [None] * 16)
+    assert [d for d in sb.batch.descs] == [descs[i] for i in sb.mine]
     dist.barrier()
     dist.destroy_process_group()
-    q.put((rank, mine, slowest))
+    q.put((rank, mine, slowest, sb.mine, flags, sub))
 
 
 def test_two_rank_gloo():
@@ -69,3 +98,7 @@ def test_two_rank_gloo():
     assert sorted(parts[0] + parts[1]) == list(range(8))
     assert not set(parts[0]) & set(parts[1])
     assert all(r[2] == 11.0 for r in res)
+    sharded = [r[3] for r in res]
+    assert sorted(sharded[0] + sharded[1]) == list(range(16))
+    for r in res:
+        assert r[4] == {i: i % 2 == 0 for i in r[3]} == r[5]
