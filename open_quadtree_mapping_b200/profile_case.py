@@ -2,6 +2,8 @@
 
     python -m open_quadtree_mapping_b200.profile_case --streams 4 --runs 3
     python -m open_quadtree_mapping_b200.profile_case --large --streams 2 --runs 1
+    ncu --profile-from-start off ... python -m open_quadtree_mapping_b200.profile_case \
+        --streams 4 --runs 1 --eager --profile-range   # only the timed run
 
 Feeds S synthetic streams (default 752x480, 64 hypotheses, 5 slots; with
 --large 1920x1080, fx=fy=1150, 128 hypotheses, 20 slots, 5-level quadtree)
@@ -23,6 +25,9 @@ def main():
     ap.add_argument("--eager", action="store_true", help="launch stage by stage, no graph")
     ap.add_argument("--large", action="store_true",
                     help="1920x1080, 128 hypotheses, 20 slots, 5-level quadtree")
+    ap.add_argument("--profile-range", action="store_true",
+                    help="bracket the timed runs with cudaProfilerStart/Stop (for ncu "
+                         "--profile-from-start off: only those runs' launches are captured)")
     args = ap.parse_args()
 
     import torch
@@ -49,12 +54,17 @@ def main():
     ext = torch.cuda.ExternalStream(b.stream_ptr())
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    if args.profile_range:
+        torch.cuda.cudart().cudaProfilerStart()
     t0 = time.perf_counter()
     e0.record(ext)
     for _ in range(args.runs):
         b.run_resident()
     e1.record(ext)
     e1.synchronize()
+    if args.profile_range:
+        torch.cuda.cudart().cudaProfilerStop()
     print("streams=%d runs=%d device_ms_per_run=%.4f wall_ms_per_run=%.4f launches_per_run=%d"
           % (args.streams, args.runs, e0.elapsed_time(e1) / args.runs,
              1000.0 * (time.perf_counter() - t0) / args.runs, b.last_launches()))
