@@ -71,9 +71,9 @@ def test_invalid_launch_shapes_are_rejected(gpu):
                 dict(col_lines=16)):
         with pytest.raises(_lib.QmError):
             b.set_tune(**bad)
-    # lines of 4096 samples: four rows per block exceed a block's shared memory
+    # lines of 4096 samples (the longest rows): at 13 bytes of shared memory
+    # per sample even four rows per block fit a block's 227 KB
     wide = BatchDepthmap([dict(width=4096, height=64, fx=2000.0, fy=2000.0, cx=2048.0, cy=32.0,
                                num_hyp=32, num_slots=1)], params=Params.for_range(32, 0.5, 50.0))
-    with pytest.raises(_lib.QmError):
-        wide.set_tune(row_warps=4)
+    wide.set_tune(row_warps=4)
     wide.set_tune(row_warps=2)

@@ -46,7 +46,13 @@ def _assert_extract_equal(g, r, comp, W, H):
     assert np.array_equal(g["labels"], ref_labels)
     assert (ref_labels >= 0).sum() > 0
     assert np.array_equal(g["sparse"], r["sparse"])
-    rel = np.abs(g["dense"] - r["dense"]) / np.abs(r["dense"])
+    # a stretch of a line cut off by zero weights (exp underflow at strong
+    # edges) that holds no sparse depth solves to 0 / 0 in both
+    gd, rd = g["dense"], r["dense"]
+    assert np.array_equal(np.isnan(gd), np.isnan(rd))
+    ok = np.isfinite(rd) & (rd != 0)
+    assert np.array_equal(gd[~ok & ~np.isnan(rd)], rd[~ok & ~np.isnan(rd)])
+    rel = np.abs(gd[ok] - rd[ok]) / np.abs(rd[ok])
     assert rel.max() < UPSAMPLE_RTOL, rel.max()
 
 

@@ -24,8 +24,8 @@ F_PX = 460.0 * W / 752.0
 
 
 def _bad_poses(T):
-    """NaN, +inf, a scaled rotation and a shear, each derived from a good
-    world->camera (or slot) pose T (12 floats)."""
+    """NaN, +inf, -inf, a rotation scaled by 2 and a shear, each derived from
+    a good world->camera (or slot) pose T (12 floats)."""
     out = []
     for k, v in ((3, np.nan), (5, np.inf), (10, -np.inf)):
         b = np.array(T, np.float32).reshape(12)
@@ -34,8 +34,9 @@ def _bad_poses(T):
     b = np.array(T, np.float32).reshape(12)
     b[[0, 1, 2, 4, 5, 6, 8, 9, 10]] *= 2.0
     out.append(b)
+    # a shear that lifts |r00| + |r01| above the bound, whatever the rotation
     b = np.array(T, np.float32).reshape(12)
-    b[1] += 1.2
+    b[1] += np.float32(1.6) * (np.float32(1.0) if b[1] >= 0 else np.float32(-1.0))
     out.append(b)
     return out
 
