@@ -57,48 +57,41 @@ __device__ __forceinline__ float *smf(int byte_off)
   return reinterpret_cast<float *>(g_smem + byte_off);
 }
 
-__host__ __device__ __forceinline__ int seg_len(int n) { return (n + 31) / 32; }
-// float pitch of a lane's segment (odd: lane-parallel accesses hit 32
-// different banks)
-__host__ __device__ __forceinline__ int seg_pitch(int n) { return seg_len(n) | 1; }
-// byte pitch of a lane's segment of image bytes: 4 x odd, so that the 32
-// lanes' bytes at the same step lie in 32 different bank words
-__host__ __device__ __forceinline__ int seg_bytes(int n) { return (((seg_len(n) + 3) / 4) | 1) * 4; }
+// Segment of a lane: m samples, m a multiple of 4 so that a segment is
+// walked in chunks of four (one 16-byte shared load or store per array and
+// chunk).  Line lengths are multiples of 8, so every segment is whole chunks.
+__host__ __device__ __forceinline__ int seg_len(int n) { return ((n + 31) / 32 + 3) & ~3; }
+// pitch of a lane's segment, in floats for the float arrays and in bytes for
+// the image bytes: 4 x odd >= m, so that the eight lanes of a 16-byte access
+// phase (and the 32 lanes of a 4-byte one) hit different banks
+__host__ __device__ __forceinline__ int seg_pitch(int n) { return 4 * ((seg_len(n) / 4) | 1); }
 __host__ __device__ __forceinline__ int farray_bytes(int n)
 {
-  return (32 * seg_pitch(n) * (int)sizeof(float) + 15) & ~15;
+  return 32 * seg_pitch(n) * (int)sizeof(float);
 }
 // bytes of one line: three float arrays (right-hand sides, pivots) and the
 // image bytes
 __host__ __device__ __forceinline__ int line_bytes(int n)
 {
-  return 3 * farray_bytes(n) + ((32 * seg_bytes(n) + 15) & ~15);
+  return 3 * farray_bytes(n) + 32 * seg_pitch(n);
 }
 
 // One line of n samples in shared memory, as byte offsets: rd / ri hold the
 // two right-hand sides (the sparse depth and its indicator), later their
 // forward values and the solution; cp the reciprocal pivots, later the
 // eliminated super-diagonal; img the line's image bytes, from which every
-// pass looks the weights up again.
+// pass looks the weights up again.  Sample k of lane l = k / m sits at
+// l * mp + k % m in each array.
 struct Line
 {
   int rd, ri, cp, img;
-  int n, m, mp, bp;
+  int n, m, mp;
   float w_close; // weight between samples n - 1 and n (the closing weight)
-  __device__ __forceinline__ int fpos(int k) const
+  __device__ __forceinline__ int pos(int k) const
   {
     const int l = k / m;
     return l * mp + (k - l * m);
   }
-  __device__ __forceinline__ int bpos(int k) const
-  {
-    const int l = k / m;
-    return l * bp + (k - l * m);
-  }
-  __device__ __forceinline__ float &RD(int p) const { return smf(rd)[p]; }
-  __device__ __forceinline__ float &RI(int p) const { return smf(ri)[p]; }
-  __device__ __forceinline__ float &CP(int p) const { return smf(cp)[p]; }
-  __device__ __forceinline__ int I(int k) const { return g_smem[img + bpos(k)]; }
 };
 
 __device__ __forceinline__ Line line_at(int base, int n, float w_close)
@@ -112,9 +105,37 @@ __device__ __forceinline__ Line line_at(int base, int n, float w_close)
   L.n = n;
   L.m = seg_len(n);
   L.mp = seg_pitch(n);
-  L.bp = seg_bytes(n);
   L.w_close = w_close;
   return L;
+}
+
+__device__ __forceinline__ float4 ld4(int arr, int p)
+{
+  return *reinterpret_cast<const float4 *>(g_smem + arr + 4 * p);
+}
+__device__ __forceinline__ void st4(int arr, int p, float4 v)
+{
+  *reinterpret_cast<float4 *>(g_smem + arr + 4 * p) = v;
+}
+// the four image bytes of samples k .. k + 3 (k a chunk start)
+__device__ __forceinline__ unsigned ldw(const Line &L, int k)
+{
+  return *reinterpret_cast<const unsigned *>(g_smem + L.img + L.pos(k));
+}
+__device__ __forceinline__ float f4(const float4 &v, int t)
+{
+  return t == 0 ? v.x : t == 1 ? v.y : t == 2 ? v.z : v.w;
+}
+__device__ __forceinline__ void set4(float4 &v, int t, float x)
+{
+  if (t == 0)
+    v.x = x;
+  else if (t == 1)
+    v.y = x;
+  else if (t == 2)
+    v.z = x;
+  else
+    v.w = x;
 }
 
 // weight between neighbours with intensities a (current) and b (previous),
@@ -136,8 +157,7 @@ __device__ __forceinline__ void build_weight_table(double sigma)
     smf(0)[t] = edge_weight<A>((float)t, 0.0f, sigma);
 }
 
-// weight between samples k - 1 and k of the line (k in 1 .. n - 1), given
-// their intensities
+// weight between samples with intensities a and b
 __device__ __forceinline__ float table_weight(int a, int b)
 {
   return smf(0)[a > b ? a - b : b - a];
@@ -172,35 +192,53 @@ __device__ __forceinline__ Mat2 shfl_up(const Mat2 &M, int off)
               __shfl_up_sync(0xffffffffu, M.c, off), __shfl_up_sync(0xffffffffu, M.d, off)};
 }
 
+// 1 / v for a positive normal v: the hardware's approximate FP64 reciprocal
+// refined by two Newton-Raphson steps r <- r + r (1 - v r), each of which
+// squares the relative error (about 2^-22 -> 2^-44 -> below 2^-53)
+__device__ __forceinline__ double recip_pos(double v)
+{
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(v));
+  double e = fma(-v, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-v, r, 1.0);
+  return fma(r, e, r);
+}
+
 struct Aff
 {
   float g, hd, hi; // z -> g z + h (two right-hand sides)
 };
 
-// Walks the weights of segment [s, e): calls f(k, wl, wr) with the weights
-// to the left and right of sample k.  w_0 = 0, w_n = the closing weight,
-// every other from the table.
+// Walks the segment [s, e) chunk by chunk: calls f(k, wl[4], wr[4]) with
+// the weights left and right of samples k .. k + 3.  w_0 = 0, w_n = the
+// closing weight, every other from the table.  The image bytes of the next
+// chunk are fetched before the current chunk is processed.
 template <class Fn>
-__device__ __forceinline__ void walk_weights(const Line &L, int s, int e, Fn &&f)
+__device__ __forceinline__ void walk_chunks(const Line &L, int s, int e, Fn &&f)
 {
   if (s >= e)
     return;
-  int Ik = L.I(s);
-  float wl = s == 0 ? 0.0f : table_weight(Ik, L.I(s - 1));
-  for (int k = s; k < e; ++k)
+  unsigned word = ldw(L, s);
+  float w0 = s == 0 ? 0.0f : table_weight((int)(word & 0xffu), g_smem[L.img + L.pos(s - 1)]);
+  for (int k = s; k < e; k += 4)
   {
-    float wr;
-    int In = 0;
-    if (k + 1 < L.n)
+    const unsigned next = k + 4 < L.n ? ldw(L, k + 4) : 0u;
+    float wl[4], wr[4];
+    int I[5];
+#pragma unroll
+    for (int t = 0; t < 4; ++t)
+      I[t] = (int)((word >> (8 * t)) & 0xffu);
+    I[4] = (int)(next & 0xffu);
+#pragma unroll
+    for (int t = 0; t < 4; ++t)
     {
-      In = L.I(k + 1);
-      wr = table_weight(In, Ik);
+      wl[t] = w0;
+      w0 = k + t + 1 == L.n ? L.w_close : table_weight(I[t + 1], I[t]);
+      wr[t] = w0;
     }
-    else
-      wr = L.w_close;
     f(k, wl, wr);
-    wl = wr;
-    Ik = In;
+    word = next;
   }
 }
 
@@ -217,10 +255,14 @@ __device__ __forceinline__ void solve_line(const Line &L, double lam)
   // entries grow by at most 1 + 2*lambda per element, far inside the double
   // range for segments of <= 128 elements, so no per-step rescaling.
   Mat2 P{1.0, 0.0, 0.0, 1.0};
-  walk_weights(L, s, e, [&](int, float wl_f, float wr_f) {
-    const double wl = wl_f, wr = wr_f;
-    const double a = -lam * wl, bb = 1.0 + lam * (wl + wr), c = -lam * wr;
-    P = Mat2{c * P.c, c * P.d, bb * P.c - a * P.a, bb * P.d - a * P.b};
+  walk_chunks(L, s, e, [&](int, const float(&wl)[4], const float(&wr)[4]) {
+#pragma unroll
+    for (int t = 0; t < 4; ++t)
+    {
+      const double a = -lam * (double)wl[t], c = -lam * (double)wr[t];
+      const double bb = 1.0 + lam * ((double)wl[t] + (double)wr[t]);
+      P = Mat2{c * P.c, c * P.d, bb * P.c - a * P.a, bb * P.d - a * P.b};
+    }
   });
   P = renorm(P);
   // inclusive scan (later segments on the left), then exclusive
@@ -244,17 +286,24 @@ __device__ __forceinline__ void solve_line(const Line &L, double lam)
   Mat2 Q{1.0, 0.0, 0.0, 1.0};
   double Dprev = 1.0;
   Aff F{1.0f, 0.0f, 0.0f};
-  walk_weights(L, s, e, [&](int k, float wl_f, float wr_f) {
+  walk_chunks(L, s, e, [&](int k, const float(&wl)[4], const float(&wr)[4]) {
     const int p = base + (k - s);
-    const double wl = wl_f, wr = wr_f;
-    const double a = -lam * wl, bb = 1.0 + lam * (wl + wr), c = -lam * wr;
-    Q = Mat2{c * Q.c, c * Q.d, bb * Q.c - a * Q.a, bb * Q.d - a * Q.b};
-    const double Dk = Q.c * z0 + Q.d;
-    const float invf = (float)(Dprev / Dk);
-    Dprev = Dk;
-    L.CP(p) = invf;
-    const float alpha = (float)(lam * wl) * invf;
-    F = Aff{alpha * F.g, alpha * F.hd + L.RD(p) * invf, alpha * F.hi + L.RI(p) * invf};
+    const float4 rd = ld4(L.rd, p), ri = ld4(L.ri, p);
+    float4 inv4;
+#pragma unroll
+    for (int t = 0; t < 4; ++t)
+    {
+      const double a = -lam * (double)wl[t], c = -lam * (double)wr[t];
+      const double bb = 1.0 + lam * ((double)wl[t] + (double)wr[t]);
+      Q = Mat2{c * Q.c, c * Q.d, bb * Q.c - a * Q.a, bb * Q.d - a * Q.b};
+      const double Dk = Q.c * z0 + Q.d;
+      const float invf = (float)(Dprev * recip_pos(Dk));
+      Dprev = Dk;
+      set4(inv4, t, invf);
+      const float alpha = (float)(lam * (double)wl[t]) * invf;
+      F = Aff{alpha * F.g, alpha * F.hd + f4(rd, t) * invf, alpha * F.hi + f4(ri, t) * invf};
+    }
+    st4(L.cp, p, inv4);
   });
 #pragma unroll
   for (int off = 1; off < 32; off <<= 1)
@@ -272,17 +321,26 @@ __device__ __forceinline__ void solve_line(const Line &L, double lam)
   // -------- forward values of the segment, eliminated super-diagonal
   // c'_k = c_k / den_k, back-substitution composition
   Aff G{1.0f, 0.0f, 0.0f};
-  walk_weights(L, s, e, [&](int k, float wl_f, float wr_f) {
+  walk_chunks(L, s, e, [&](int k, const float(&wl)[4], const float(&wr)[4]) {
     const int p = base + (k - s);
-    const float invf = L.CP(p);
-    const float alpha = (float)(lam * (double)wl_f) * invf;
-    const float cpk = (float)(-lam * (double)wr_f * (double)invf);
-    dprev = alpha * dprev + L.RD(p) * invf;
-    iprev = alpha * iprev + L.RI(p) * invf;
-    L.RD(p) = dprev;
-    L.RI(p) = iprev;
-    L.CP(p) = cpk;
-    G = Aff{-G.g * cpk, G.g * dprev + G.hd, G.g * iprev + G.hi};
+    const float4 inv4 = ld4(L.cp, p);
+    float4 rd = ld4(L.rd, p), ri = ld4(L.ri, p), cp4;
+#pragma unroll
+    for (int t = 0; t < 4; ++t)
+    {
+      const float invf = f4(inv4, t);
+      const float alpha = (float)(lam * (double)wl[t]) * invf;
+      const float cpk = (float)(-lam * (double)wr[t] * (double)invf);
+      dprev = alpha * dprev + f4(rd, t) * invf;
+      iprev = alpha * iprev + f4(ri, t) * invf;
+      set4(rd, t, dprev);
+      set4(ri, t, iprev);
+      set4(cp4, t, cpk);
+      G = Aff{-G.g * cpk, G.g * dprev + G.hd, G.g * iprev + G.hi};
+    }
+    st4(L.rd, p, rd);
+    st4(L.ri, p, ri);
+    st4(L.cp, p, cp4);
   });
   // suffix scan: lane l composes with the segments after it
 #pragma unroll
@@ -298,18 +356,28 @@ __device__ __forceinline__ void solve_line(const Line &L, double lam)
   float zi = __shfl_down_sync(0xffffffffu, G.hi, 1);
   if (lane == 31)
     zd = zi = 0.0f;
-  // -------- back substitution of the segment
-  for (int k = e - 1; k >= s; --k)
+  // -------- back substitution of the segment, chunk by chunk from the end
+  for (int k = e - 4; k >= s; k -= 4)
   {
     const int p = base + (k - s);
-    const float cpk = L.CP(p);
-    zd = L.RD(p) - cpk * zd;
-    zi = L.RI(p) - cpk * zi;
-    L.RD(p) = zd;
-    L.RI(p) = zi;
+    const float4 cp4 = ld4(L.cp, p);
+    float4 rd = ld4(L.rd, p), ri = ld4(L.ri, p);
+#pragma unroll
+    for (int t = 3; t >= 0; --t)
+    {
+      zd = f4(rd, t) - f4(cp4, t) * zd;
+      zi = f4(ri, t) - f4(cp4, t) * zi;
+      set4(rd, t, zd);
+      set4(ri, t, zi);
+    }
+    st4(L.rd, p, rd);
+    st4(L.ri, p, ri);
   }
   __syncwarp();
 }
+
+// elements one lane loads before it stores them (global loads in flight)
+constexpr int kLoadBatch = 8;
 
 template <class A>
 __global__ void __launch_bounds__(kMaxRowWarps * 32)
@@ -334,23 +402,38 @@ __global__ void __launch_bounds__(kMaxRowWarps * 32)
   // previous frame's update left them set); coalesced stores in a
   // latency-bound pass
   unsigned long long *zk = J.zkey ? J.zkey + (size_t)y * W : nullptr;
-  for (int k = lane; k < n; k += 32)
+  for (int k0 = lane; k0 < n; k0 += 32 * kLoadBatch)
   {
-    const int p = L.fpos(k);
-    if (zk)
-      zk[k] = ~0ull;
-    g_smem[L.img + L.bpos(k)] = img[k];
-    const float d = sp[k];
-    L.RD(p) = d;
-    L.RI(p) = d > 0.0f ? 1.0f : 0.0f;
+    uint8_t iv[kLoadBatch];
+    float dv[kLoadBatch];
+#pragma unroll
+    for (int u = 0; u < kLoadBatch; ++u)
+    {
+      const int k = k0 + 32 * u;
+      iv[u] = k < n ? img[k] : 0;
+      dv[u] = k < n ? sp[k] : 0.0f;
+    }
+#pragma unroll
+    for (int u = 0; u < kLoadBatch; ++u)
+    {
+      const int k = k0 + 32 * u;
+      if (k >= n)
+        break;
+      if (zk)
+        zk[k] = ~0ull;
+      const int p = L.pos(k);
+      g_smem[L.img + p] = iv[u];
+      smf(L.rd)[p] = dv[u];
+      smf(L.ri)[p] = dv[u] > 0.0f ? 1.0f : 0.0f;
+    }
   }
   __syncwarp();
   solve_line(L, kp.up_lambda);
   float2 *out = J.rowres + (size_t)y * W;
   for (int k = lane; k < n; k += 32)
   {
-    const int p = L.fpos(k);
-    out[k] = make_float2(L.RD(p), L.RI(p));
+    const int p = L.pos(k);
+    out[k] = make_float2(smf(L.rd)[p], smf(L.ri)[p]);
   }
 }
 
@@ -367,19 +450,35 @@ __global__ void __launch_bounds__(kMaxColLines * 32)
   const int x0 = lb * lines;
   const int n = H / 8 * 8;
   const int per_line = line_bytes(max_n);
-  // cooperative stripe load: row k, column x0 + c
-  for (int t = threadIdx.x; t < n * lines; t += blockDim.x)
+  const int total = n * lines;
+  // cooperative stripe load: row k, column x0 + c; a batch of loads per
+  // thread in flight before their shared-memory stores
+  for (int t0 = threadIdx.x; t0 < total; t0 += (int)blockDim.x * kLoadBatch)
   {
-    const int k = t / lines, c = t - k * lines;
-    const int x = x0 + c;
-    if (x >= W)
-      continue;
-    const Line L = line_at(kTableBytes + c * per_line, n, 0.0f);
-    const int p = L.fpos(k);
-    const float2 r = J.rowres[(size_t)k * W + x];
-    L.RD(p) = r.x;
-    L.RI(p) = r.y;
-    g_smem[L.img + L.bpos(k)] = J.ref[(size_t)k * J.ref_pitch + x];
+    float2 rv[kLoadBatch];
+    uint8_t iv[kLoadBatch];
+#pragma unroll
+    for (int u = 0; u < kLoadBatch; ++u)
+    {
+      const int t = t0 + u * (int)blockDim.x;
+      const int k = t / lines, x = x0 + (t - k * lines);
+      const bool in = t < total && x < W;
+      rv[u] = in ? J.rowres[(size_t)k * W + x] : make_float2(0.0f, 0.0f);
+      iv[u] = in ? J.ref[(size_t)k * J.ref_pitch + x] : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < kLoadBatch; ++u)
+    {
+      const int t = t0 + u * (int)blockDim.x;
+      const int k = t / lines, c = t - k * lines;
+      if (t >= total || x0 + c >= W)
+        continue;
+      const Line L = line_at(kTableBytes + c * per_line, n, 0.0f);
+      const int p = L.pos(k);
+      smf(L.rd)[p] = rv[u].x;
+      smf(L.ri)[p] = rv[u].y;
+      g_smem[L.img + p] = iv[u];
+    }
   }
   __syncthreads();
   const int x = x0 + warp;
@@ -392,15 +491,15 @@ __global__ void __launch_bounds__(kMaxColLines * 32)
     solve_line(line_at(kTableBytes + warp * per_line, n, w_close), kp.up_lambda);
   }
   __syncthreads();
-  for (int t = threadIdx.x; t < n * lines; t += blockDim.x)
+  for (int t = threadIdx.x; t < total; t += blockDim.x)
   {
     const int k = t / lines, c = t - k * lines;
     const int xc = x0 + c;
     if (xc >= W)
       continue;
     const Line L = line_at(kTableBytes + c * per_line, n, 0.0f);
-    const int p = L.fpos(k);
-    J.dense[(size_t)k * W + xc] = A::div(L.RD(p), L.RI(p));
+    const int p = L.pos(k);
+    J.dense[(size_t)k * W + xc] = A::div(smf(L.rd)[p], smf(L.ri)[p]);
   }
 }
 
