@@ -73,7 +73,8 @@ std::vector<int> stage_blocks(const Shape &s, const JobLayout &lay, const qm_par
   b[st.extract()] = cdiv((long)lay.lw[0] * lay.lh[0], epb);
   b[st.row()] = cdiv(s.H, tune.row_warps);
   b[st.col()] = cdiv(s.W, tune.col_lines);
-  b[st.ftrans()] = b[st.fupd()] = cdiv((long)s.W * s.H, kFlatThreads);
+  b[st.ftrans()] = cdiv((long)s.W * s.H, kFlatThreads * kFuseTransformPx);
+  b[st.fupd()] = cdiv((long)s.W * s.H, kFlatThreads * kFuseUpdatePx);
   return b;
 }
 

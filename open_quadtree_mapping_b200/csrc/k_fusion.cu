@@ -70,21 +70,28 @@ __device__ __forceinline__ double recip_pos(double v)
   return fma(r, e, r);
 }
 
-template <class A>
-__global__ void __launch_bounds__(kFlatThreads)
-    k_fuse_transform(const __grid_constant__ Batch B)
+// pixel idx of a W-wide image: (x, y) without an integer division (idx <
+// 2^24 is exact in float; the float quotient is off by at most one row)
+__device__ __forceinline__ void pixel_xy(int idx, int W, float inv_w, int &x, int &y)
 {
-  int lb;
-  const JobDesc &J = job_of(B, lb);
+  y = (int)((float)idx * inv_w);
+  if (y * W > idx)
+    --y;
+  else if ((y + 1) * W <= idx)
+    ++y;
+  x = idx - y * W;
+}
+
+// Moves one seed into the current frame and enters it in the z-buffer.
+template <class A>
+__device__ __forceinline__ void transform_px(const JobDesc &J, int idx, float4 info, float inv_w)
+{
   const int W = J.W, H = J.H;
-  const int idx = lb * blockDim.x + threadIdx.x;
-  if (idx >= W * H)
-    return;
-  const int x = idx % W, y = idx / W;
-  float4 info = J.seeds_in[idx];
   // is_badpoint (depth_fusion.cu:25-28)
   if (info.x < 0.001 || A::div(info.x, info.x + info.y) < 0.45)
     return;
+  int x, y;
+  pixel_xy(idx, W, inv_w, x, y);
   const Cam cam{J.fx, J.fy, J.cx, J.cy};
   const float3 dir = A::ray((float)x, (float)y, cam);
   float T[12];
@@ -113,26 +120,44 @@ __global__ void __launch_bounds__(kFlatThreads)
   }
 }
 
+// kFuseTransformPx pixels per thread, their seeds loaded before any is
+// processed (the loads are the latency that bounds this pass)
+template <class A>
 __global__ void __launch_bounds__(kFlatThreads)
-    k_fuse_update(const __grid_constant__ Batch B)
+    k_fuse_transform(const __grid_constant__ Batch B)
 {
   int lb;
   const JobDesc &J = job_of(B, lb);
+  const int npx = J.W * J.H;
+  const int base = lb * (int)blockDim.x * kFuseTransformPx + (int)threadIdx.x;
+  const float inv_w = 1.0f / (float)J.W;
+  float4 info[kFuseTransformPx];
+#pragma unroll
+  for (int u = 0; u < kFuseTransformPx; ++u)
+  {
+    const int idx = base + u * (int)blockDim.x;
+    info[u] = idx < npx ? J.seeds_in[idx] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  }
+#pragma unroll
+  for (int u = 0; u < kFuseTransformPx; ++u)
+  {
+    const int idx = base + u * (int)blockDim.x;
+    if (idx < npx)
+      transform_px<A>(J, idx, info[u], inv_w);
+  }
+}
+
+// hole filling (hole_filling, depth_fusion.cu:121-144): the pixel's own key,
+// or for an empty pixel the smallest key of its propagating 3x3 neighbours;
+// returns the source seed index (0 = none)
+__device__ __forceinline__ int resolve_source(const JobDesc &J, int idx, unsigned long long key,
+                                              float inv_w)
+{
   const int W = J.W, H = J.H;
-  const int idx = lb * blockDim.x + threadIdx.x;
-  if (idx >= W * H)
-    return;
-  const double dep = (double)J.dense[idx];
-  double unc = fmax(0.5, dep * 0.2);
-  unc *= unc;
-  if (dep <= 0.0)
-    unc = 1e9;
-  // hole filling (hole_filling, depth_fusion.cu:121-144): the pixel's own key, or
-  // for an empty pixel the smallest key of its propagating 3x3 neighbours
-  const int x = idx % W, y = idx / W;
-  unsigned long long key = J.zkey[idx];
   if (key == kEmpty)
   {
+    int x, y;
+    pixel_xy(idx, W, inv_w, x, y);
     for (int i = -1; i <= 1; ++i)
       for (int jx = -1; jx <= 1; ++jx)
       {
@@ -143,13 +168,23 @@ __global__ void __launch_bounds__(kFlatThreads)
         key = k < key ? k : key;
       }
   }
-  const int pre = key == kEmpty ? 0 : (int)(unsigned)(key & 0xffffffffull);
+  return key == kEmpty ? 0 : (int)(unsigned)(key & 0xffffffffull);
+}
+
+// fuse_currentmap (depth_fusion.cu:146-213) of one pixel in FP64, given its
+// upsampled depth and its prior seed (source pre > 0) or none
+__device__ __forceinline__ void update_px(const JobDesc &J, int idx, double dep, int pre,
+                                          float4 s)
+{
+  double unc = fmax(0.5, dep * 0.2);
+  unc *= unc;
+  if (dep <= 0.0)
+    unc = 1e9;
   if (J.table)
     J.table[idx] = pre;
   double a, b, mu, s2;
   if (pre > 0)
   {
-    const float4 s = J.seeds_in[pre];
     a = s.x;
     b = s.y;
     mu = s.z;
@@ -206,6 +241,43 @@ __global__ void __launch_bounds__(kFlatThreads)
   const double b_p = q * (1.0 - f);
   J.dense[idx] = (ratio > 0.60) ? (float)mu_p : -1.0f;
   J.seeds_out[idx] = make_float4((float)a_p, (float)b_p, (float)mu_p, (float)s2_p);
+}
+
+// kFuseUpdatePx pixels per thread: depths and keys first, then the sources,
+// then the source seeds (a dependent load), then the updates
+__global__ void __launch_bounds__(kFlatThreads)
+    k_fuse_update(const __grid_constant__ Batch B)
+{
+  int lb;
+  const JobDesc &J = job_of(B, lb);
+  const int npx = J.W * J.H;
+  const int base = lb * (int)blockDim.x * kFuseUpdatePx + (int)threadIdx.x;
+  const float inv_w = 1.0f / (float)J.W;
+  float dep[kFuseUpdatePx];
+  unsigned long long key[kFuseUpdatePx];
+#pragma unroll
+  for (int u = 0; u < kFuseUpdatePx; ++u)
+  {
+    const int idx = base + u * (int)blockDim.x;
+    dep[u] = idx < npx ? J.dense[idx] : 0.0f;
+    key[u] = idx < npx ? J.zkey[idx] : kEmpty;
+  }
+  int pre[kFuseUpdatePx];
+  float4 src[kFuseUpdatePx];
+#pragma unroll
+  for (int u = 0; u < kFuseUpdatePx; ++u)
+  {
+    const int idx = base + u * (int)blockDim.x;
+    pre[u] = idx < npx ? resolve_source(J, idx, key[u], inv_w) : 0;
+    src[u] = pre[u] > 0 ? J.seeds_in[pre[u]] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  }
+#pragma unroll
+  for (int u = 0; u < kFuseUpdatePx; ++u)
+  {
+    const int idx = base + u * (int)blockDim.x;
+    if (idx < npx)
+      update_px(J, idx, (double)dep[u], pre[u], src[u]);
+  }
 }
 
 // sigma^2 of every seed (the fused variance)
