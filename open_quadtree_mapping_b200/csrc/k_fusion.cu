@@ -243,7 +243,9 @@ __device__ __forceinline__ void update_px(const JobDesc &J, int idx, double dep,
   J.seeds_out[idx] = make_float4((float)a_p, (float)b_p, (float)mu_p, (float)s2_p);
 }
 
-// kFuseUpdatePx pixels per thread: depths and keys first, then the sources,
+// kFuseUpdatePx pixels per thread (one: the update is FP64- and issue-bound,
+// and two per thread measured slower at the lower occupancy): depths and
+// keys first, then the sources,
 // then the source seeds (a dependent load), then the updates
 __global__ void __launch_bounds__(kFlatThreads)
     k_fuse_update(const __grid_constant__ Batch B)

@@ -91,7 +91,7 @@ void launch_col_solve(const Batch &B, int blocks, KParams kp, int arith, int max
 // pixels per thread of the fusion transform and update (their blocks cover
 // kFlatThreads times as many)
 constexpr int kFuseTransformPx = 4;
-constexpr int kFuseUpdatePx = 2;
+constexpr int kFuseUpdatePx = 1;
 void launch_fuse_transform(const Batch &B, int blocks, int arith, cudaStream_t s);
 // hole filling + posterior update (reads the z-buffer keys, leaves them set:
 // the next frame's row solve resets them)
