@@ -89,6 +89,7 @@ _SIGS = {
     "qm_depthmap_set_semidense": (_I, [_P, _I]),
     "qm_batch_set_group_bytes": (_I, [_P, _S]),
     "qm_batch_set_coarse_bp": (_I, [_P, _I]),
+    "qm_batch_set_stagger": (_I, [_P, _I]),
     "qm_batch_set_autotune": (_I, [_P, _I]),
     "qm_batch_set_tune": (_I, [_P, ctypes.POINTER(_I)]),
     "qm_batch_get_tune": (_I, [_P, ctypes.POINTER(_I)]),

@@ -878,6 +878,15 @@ int qm_batch_set_coarse_bp(qm_batch *b, int max_cells)
   });
 }
 
+int qm_batch_set_stagger(qm_batch *b, int enable)
+{
+  return guarded([&] {
+    require(b != nullptr, "NULL handle");
+    std::lock_guard<std::mutex> lock(b->set->mutex());
+    b->set->engine().set_stagger(enable != 0);
+  });
+}
+
 int qm_batch_set_autotune(qm_batch *b, int enable)
 {
   return guarded([&] {

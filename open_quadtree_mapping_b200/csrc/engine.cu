@@ -464,6 +464,7 @@ struct Plan
   bool tuned = false;                  // launch shapes settled (timed or fixed)
   size_t group_bytes = 0;              // the job grouping the graphs were captured with
   int coarse_cells = 0;                // the coarse-level threshold they were captured with
+  bool stagger = false;                // the branch staggering they were captured with
   cudaGraphExec_t exec[2] = {nullptr, nullptr}; // by step parity
   StageTable &table() { return tb->table; }
   void drop_graphs()
@@ -512,6 +513,7 @@ Engine::Engine(int device, const qm_params &p, const std::vector<Shape> &shapes)
   {
     check(cudaStreamCreateWithFlags(&branch_[i], cudaStreamNonBlocking), "cudaStreamCreate");
     check(cudaEventCreateWithFlags(&ev_join_[i], cudaEventDisableTiming), "cudaEventCreate");
+    check(cudaEventCreateWithFlags(&ev_stage_[i], cudaEventDisableTiming), "cudaEventCreate");
   }
   check(cudaEventCreate(&ev0_), "cudaEventCreate");
   check(cudaEventCreate(&ev1_), "cudaEventCreate");
@@ -638,6 +640,8 @@ Engine::~Engine()
     }
     if (ev_join_[i])
       cudaEventDestroy(ev_join_[i]);
+    if (ev_stage_[i])
+      cudaEventDestroy(ev_stage_[i]);
   }
   if (ev_fork_)
     cudaEventDestroy(ev_fork_);
@@ -709,7 +713,8 @@ Plan &Engine::plan_for(const std::vector<int> &active)
   if (it != plans_.end())
   {
     Plan &pl = *it->second;
-    if (pl.group_bytes != group_bytes_ || pl.coarse_cells != coarse_cells_)
+    if (pl.group_bytes != group_bytes_ || pl.coarse_cells != coarse_cells_ ||
+        pl.stagger != stagger_)
       pl.drop_graphs();
     return pl;
   }
@@ -898,6 +903,7 @@ int Engine::enqueue(Plan &pl, cudaStream_t s)
   const Stages st{params_.bp_levels};
   pl.group_bytes = group_bytes_;
   pl.coarse_cells = coarse_cells_;
+  pl.stagger = stagger_;
   const int n = (int)pl.active.size();
   const int k = std::min(branches_, n);
   if (k < 2)
@@ -906,15 +912,29 @@ int Engine::enqueue(Plan &pl, cudaStream_t s)
   // k independent branches over consecutive ranges of the jobs (every stage
   // is per job): the GPU fills the latency-bound stretches of one branch
   // (coarse BP levels, line solves) with the other branches' work
+  // Staggered (the default): branch i + 1 starts when branch i's cost
+  // volume is done, so that cost kernels (bound by instruction issue) run
+  // beside the previous branch's BP half-sweeps (bound by HBM bandwidth)
+  // instead of beside each other.
   check(cudaEventRecord(ev_fork_, s), "fork");
   int nl = 0;
   for (int i = 0; i < k; ++i)
   {
     cudaStream_t bs = i == 0 ? s : branch_[i - 1];
+    const int ja = n * i / k, jb = n * (i + 1) / k;
     if (i > 0)
-      check(cudaStreamWaitEvent(bs, ev_fork_, 0), "fork");
-    nl += enqueue_range(B, pl.table(), params_, group_bytes_, coarse_cells_, 0, st.count() - 1,
-                        bs, nullptr, n * i / k, n * (i + 1) / k);
+      check(cudaStreamWaitEvent(bs, stagger_ ? ev_stage_[i - 1] : ev_fork_, 0), "fork");
+    if (stagger_ && i + 1 < k)
+    {
+      nl += enqueue_range(B, pl.table(), params_, group_bytes_, coarse_cells_, 0, st.cost(), bs,
+                          nullptr, ja, jb);
+      check(cudaEventRecord(ev_stage_[i], bs), "stage");
+      nl += enqueue_range(B, pl.table(), params_, group_bytes_, coarse_cells_, st.cost() + 1,
+                          st.count() - 1, bs, nullptr, ja, jb);
+    }
+    else
+      nl += enqueue_range(B, pl.table(), params_, group_bytes_, coarse_cells_, 0, st.count() - 1,
+                          bs, nullptr, ja, jb);
   }
   for (int i = 1; i < k; ++i)
   {

@@ -194,6 +194,12 @@ public:
   // cluster launch; 0: one launch per half-sweep at every level.  Results
   // do not depend on it.
   void set_coarse_cells(int cells) { coarse_cells_ = cells < 0 ? 0 : cells; }
+  // true: branch i + 1 starts once branch i's cost volume is done, so the
+  // issue-bound cost kernel of one branch runs beside the bandwidth-bound
+  // BP of the previous one; false: all branches start together.  Results do
+  // not depend on it.
+  void set_stagger(bool on) { stagger_ = on; }
+  bool stagger() const { return stagger_; }
   int coarse_cells() const { return coarse_cells_; }
   int last_launches() const { return last_launches_; }
   // 1: the sparse buffers arrive filled with the semi-dense tracker's depths
@@ -252,6 +258,8 @@ private:
   cudaStream_t stream_ = nullptr;
   cudaStream_t branch_[kMaxBranches - 1] = {}; // streams of branches 2..k
   cudaEvent_t ev_fork_ = nullptr, ev_join_[kMaxBranches - 1] = {};
+  cudaEvent_t ev_stage_[kMaxBranches - 1] = {}; // branch i's cost stage done
+  bool stagger_ = true;
   int branches_ = QM_DEFAULT_BRANCHES;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
   bool graphs_ = true;

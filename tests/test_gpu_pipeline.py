@@ -102,6 +102,12 @@ def test_batch_equals_plain_and_graph_equals_eager(gpu):
     coarse_off.set_coarse_bp(0)
     coarse_all = BatchDepthmap([_stream_kw()] * 3, params=p)
     coarse_all.set_coarse_bp(1 << 30)
+    # branches started together instead of staggered behind each other's
+    # cost volume, and three branches
+    unstaggered = BatchDepthmap([_stream_kw()] * 3, params=p)
+    unstaggered.set_stagger(False)
+    three = BatchDepthmap([_stream_kw()] * 3, params=p)
+    three.set_branches(3)
     singles = [BatchDepthmap([_stream_kw()], params=p) for _ in range(3)]
     for i in range(14):
         imgs = [s[0][i] for s in seqs]
@@ -113,6 +119,8 @@ def test_batch_equals_plain_and_graph_equals_eager(gpu):
         assert branched.add_frames(imgs, poses) == hb
         assert coarse_off.add_frames(imgs, poses) == hb
         assert coarse_all.add_frames(imgs, poses) == hb
+        assert unstaggered.add_frames(imgs, poses) == hb
+        assert three.add_frames(imgs, poses) == hb
         hs = [singles[k].add_frames([imgs[k]], [poses[k]])[0] for k in range(3)]
         assert hb == he == hs
         if all(hb) and i > 0:
@@ -126,6 +134,8 @@ def test_batch_equals_plain_and_graph_equals_eager(gpu):
                 assert np.array_equal(a, branched.get_depth(k))
                 assert np.array_equal(a, coarse_off.get_depth(k))
                 assert np.array_equal(a, coarse_all.get_depth(k))
+                assert np.array_equal(a, unstaggered.get_depth(k))
+                assert np.array_equal(a, three.get_depth(k))
                 assert np.array_equal(batch.get_debug(k), coarse_off.get_debug(k))
                 assert np.array_equal(a, singles[k].get_depth(0))
                 assert np.array_equal(batch.get_debug(k), singles[k].get_debug(0))
