@@ -215,10 +215,11 @@ int qm_batch_set_group_bytes(qm_batch *b, size_t bytes);
  * launch per half-sweep everywhere; default 4096.  Results do not depend on
  * it. */
 int qm_batch_set_coarse_bp(qm_batch *b, int max_cells);
-/* 1 (the default) = with two or more branches, branch i + 1 starts once
- * branch i's cost volume is done, so the issue-bound cost kernel of one
- * branch overlaps the bandwidth-bound belief propagation of the previous
- * one; 0 = all branches start together.  Results do not depend on it. */
+/* 1 = with two or more branches, branch i + 1 starts once branch i's cost
+ * volume is done, so the issue-bound cost kernel of one branch overlaps the
+ * bandwidth-bound belief propagation of the previous one; 0 (the default,
+ * measured faster) = all branches start together.  Results do not depend
+ * on it. */
 int qm_batch_set_stagger(qm_batch *b, int enable);
 /* Launch shapes of the BP and line-solver kernels: warps per block of the
  * BP half-sweeps and of the extraction (4, 8 or 16), rows per block of the

@@ -912,10 +912,10 @@ int Engine::enqueue(Plan &pl, cudaStream_t s)
   // k independent branches over consecutive ranges of the jobs (every stage
   // is per job): the GPU fills the latency-bound stretches of one branch
   // (coarse BP levels, line solves) with the other branches' work
-  // Staggered (the default): branch i + 1 starts when branch i's cost
-  // volume is done, so that cost kernels (bound by instruction issue) run
-  // beside the previous branch's BP half-sweeps (bound by HBM bandwidth)
-  // instead of beside each other.
+  // Staggered (optional): branch i + 1 starts when branch i's cost volume
+  // is done, so that cost kernels (bound by instruction issue) run beside
+  // the previous branch's BP half-sweeps (bound by HBM bandwidth) instead of
+  // beside each other.
   check(cudaEventRecord(ev_fork_, s), "fork");
   int nl = 0;
   for (int i = 0; i < k; ++i)

@@ -196,8 +196,9 @@ public:
   void set_coarse_cells(int cells) { coarse_cells_ = cells < 0 ? 0 : cells; }
   // true: branch i + 1 starts once branch i's cost volume is done, so the
   // issue-bound cost kernel of one branch runs beside the bandwidth-bound
-  // BP of the previous one; false: all branches start together.  Results do
-  // not depend on it.
+  // BP of the previous one; false (the default; measured faster on a B200:
+  // 2.91 vs 2.97 ms per 32 x 752x480 batch with two branches): all
+  // branches start together.  Results do not depend on it.
   void set_stagger(bool on) { stagger_ = on; }
   bool stagger() const { return stagger_; }
   int coarse_cells() const { return coarse_cells_; }
@@ -259,7 +260,7 @@ private:
   cudaStream_t branch_[kMaxBranches - 1] = {}; // streams of branches 2..k
   cudaEvent_t ev_fork_ = nullptr, ev_join_[kMaxBranches - 1] = {};
   cudaEvent_t ev_stage_[kMaxBranches - 1] = {}; // branch i's cost stage done
-  bool stagger_ = true;
+  bool stagger_ = false;
   int branches_ = QM_DEFAULT_BRANCHES;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
   bool graphs_ = true;

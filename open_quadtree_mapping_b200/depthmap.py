@@ -301,7 +301,7 @@ class BatchDepthmap:
         _lib.check(_lib.lib().qm_batch_set_coarse_bp(self._h, int(max_cells)))
 
     def set_stagger(self, on: bool) -> None:
-        """Branch i + 1 starts after branch i's cost volume (default on)."""
+        """Branch i + 1 starts after branch i's cost volume (default off)."""
         _lib.check(_lib.lib().qm_batch_set_stagger(self._h, 1 if on else 0))
 
     TUNE_FIELDS = ("sweep_warps", "extract_warps", "row_warps", "col_lines")

@@ -102,10 +102,10 @@ def test_batch_equals_plain_and_graph_equals_eager(gpu):
     coarse_off.set_coarse_bp(0)
     coarse_all = BatchDepthmap([_stream_kw()] * 3, params=p)
     coarse_all.set_coarse_bp(1 << 30)
-    # branches started together instead of staggered behind each other's
-    # cost volume, and three branches
-    unstaggered = BatchDepthmap([_stream_kw()] * 3, params=p)
-    unstaggered.set_stagger(False)
+    # branches staggered behind each other's cost volume instead of started
+    # together, and three branches
+    staggered = BatchDepthmap([_stream_kw()] * 3, params=p)
+    staggered.set_stagger(True)
     three = BatchDepthmap([_stream_kw()] * 3, params=p)
     three.set_branches(3)
     singles = [BatchDepthmap([_stream_kw()], params=p) for _ in range(3)]
@@ -119,7 +119,7 @@ def test_batch_equals_plain_and_graph_equals_eager(gpu):
         assert branched.add_frames(imgs, poses) == hb
         assert coarse_off.add_frames(imgs, poses) == hb
         assert coarse_all.add_frames(imgs, poses) == hb
-        assert unstaggered.add_frames(imgs, poses) == hb
+        assert staggered.add_frames(imgs, poses) == hb
         assert three.add_frames(imgs, poses) == hb
         hs = [singles[k].add_frames([imgs[k]], [poses[k]])[0] for k in range(3)]
         assert hb == he == hs
@@ -134,7 +134,7 @@ def test_batch_equals_plain_and_graph_equals_eager(gpu):
                 assert np.array_equal(a, branched.get_depth(k))
                 assert np.array_equal(a, coarse_off.get_depth(k))
                 assert np.array_equal(a, coarse_all.get_depth(k))
-                assert np.array_equal(a, unstaggered.get_depth(k))
+                assert np.array_equal(a, staggered.get_depth(k))
                 assert np.array_equal(a, three.get_depth(k))
                 assert np.array_equal(batch.get_debug(k), coarse_off.get_debug(k))
                 assert np.array_equal(a, singles[k].get_depth(0))
