@@ -188,12 +188,8 @@ int enqueue_range(const Batch &B, const StageTable &T, const qm_params &p, size_
   };
   all(kQuadtree, st.qt(), [&](const Batch &b, int g) { launch_quadtree(b, g, kp, s); });
   const int max_d = T.dvals.empty() ? 0 : T.dvals.back();
-  // when the cost volume and the first pyramid level are enqueued together,
-  // the cost kernel writes level 1 from its tiles (no level-1 pass)
-  const int l1_in_cost = (L > 1 && in(st.cost()) && in(st.pyr(1))) ? 1 : 0;
-  all(kCost, st.cost(),
-      [&](const Batch &b, int g) { launch_cost(b, g, ar, max_d, s, l1_in_cost); });
-  for (int l = 1 + l1_in_cost; l < L; ++l)
+  all(kCost, st.cost(), [&](const Batch &b, int g) { launch_cost(b, g, ar, max_d, s); });
+  for (int l = 1; l < L; ++l)
     all(kPyramid, st.pyr(l), [&](const Batch &b, int g) { launch_pyramid(b, g, l, s); });
   // BP, coarse to fine.  The top levels lc..L-1 whose cells are few (and
   // which have two or more half-sweeps) run as one cluster launch per

@@ -1,8 +1,7 @@
 // Multi-view matching cost at quadtree nodes (image_to_cost +
 // normalize_the_cost, depth_extract.cu:135-244 of the reference).
 //
-// A block owns a tile of kCostTileW cells of two consecutive cell rows
-// (kCostCells = 32 cells; level-1 pyramid cells are whole inside it).  Warp
+// A block owns a tile of kCostCells consecutive cells of one cell row.  Warp
 // 0 finds the tile's node cells (ballot) and stages, per node, its ray and
 // 3x3 reference patch in shared memory; the block also stages the slot poses
 // and the hypothesis depths.  Thread t then owns node t % n (n nodes in the
@@ -14,10 +13,7 @@
 // an integer intensity difference, so the sum is exact and equal to the
 // reference's shared-memory tree over slots.  The projection follows the
 // reference's arithmetic (ArithRef) or IEEE rounding (ArithIeee).  The tile's
-// costs are assembled in shared memory and written as one contiguous run per
-// row; in the batched pipeline the block then also writes the level-1
-// pyramid cells of its tile (the sums of their 2x2 children), so the level-0
-// costs are not read back for them.
+// costs are assembled in shared memory and written as one contiguous run.
 //
 // Cells that are not node origins, or touch the border (x <= 0, y <= 0,
 // x >= W-1, y >= H-1), get cost 0 for every hypothesis, as the reference's
@@ -73,7 +69,7 @@ __device__ __forceinline__ void patch_axis(float u, float a, float b, float (&c)
 // 2.29 ms per 2 streams at 5 blocks, 2.65 ms at 60 registers).
 template <class A>
 __global__ void __launch_bounds__(kFlatThreads, 5)
-    k_cost(const __grid_constant__ Batch B, int write_l1)
+    k_cost(const __grid_constant__ Batch B)
 {
   // costs of the tile, [kCostCells][D + 1] (the padding keeps lanes that
   // store one hypothesis of different cells on different banks)
@@ -90,11 +86,9 @@ __global__ void __launch_bounds__(kFlatThreads, 5)
   int lb;
   const JobDesc &J = job_of(B, lb);
   const int D = J.D, F = J.F, W = J.W, H = J.H;
-  // the tile: kCostTileW cells of two consecutive cell rows (cy0 even)
-  const int segs = (J.cw + kCostTileW - 1) / kCostTileW;
-  const int ty = lb / segs;
-  const int cy0 = 2 * ty, cx0 = (lb - ty * segs) * kCostTileW;
-  const int tw = min(kCostTileW, J.cw - cx0), th = min(2, J.ch - cy0);
+  const int segs = (J.cw + kCostCells - 1) / kCostCells;
+  const int cy = lb / segs, cx0 = (lb - cy * segs) * kCostCells;
+  const int ncells = min(kCostCells, J.cw - cx0);
   const int tid = threadIdx.x;
   // the job's (deduplicated) slots and the hypothesis depths, once per block
   for (int i = tid; i < F * 12; i += blockDim.x)
@@ -107,17 +101,15 @@ __global__ void __launch_bounds__(kFlatThreads, 5)
   for (int d = tid; d < D; d += blockDim.x)
     s_depth[d] = A::hyp_depth(J.step, J.min_inv, d);
   const int sd = D + 1;
-  for (int i = tid; i < kCostCells * sd; i += blockDim.x)
+  for (int i = tid; i < ncells * sd; i += blockDim.x)
     s_out[i] = 0.0f;
   const Cam cam{J.fx, J.fy, J.cx, J.cy};
   if (tid < 32)
   {
-    // node test of tile cell tid (column tid % kCostTileW of row tid /
-    // kCostTileW): quadtree node origin away from the border
-    const int tc = tid % kCostTileW, tr = tid / kCostTileW;
-    const int x = (cx0 + tc) * 4, y = (cy0 + tr) * 4;
+    // node test of cell cx0 + tid: quadtree node origin away from the border
+    const int x = (cx0 + tid) * 4, y = cy * 4;
     bool node = false;
-    if (tc < tw && tr < th && x > 0 && y > 0 && x < W - 1 && y < H - 1)
+    if (tid < ncells && x > 0 && y > 0 && x < W - 1 && y < H - 1)
     {
       const int size = 1 << J.levels[(size_t)y * W + x];
       node = x % size == 0 && y % size == 0;
@@ -207,52 +199,26 @@ __global__ void __launch_bounds__(kFlatThreads, 5)
     }
   }
   __syncthreads();
-  // each tile row's cells are consecutive in the [cell][D] layout
-  for (int r = 0; r < th; ++r)
+  // the tile's cells are consecutive in the [cell][D] layout
+  float *out = J.lv[0].data + ((size_t)cy * J.cw + cx0) * D;
+  for (int i = tid; i < ncells * D; i += blockDim.x)
   {
-    float *out = J.lv[0].data + ((size_t)(cy0 + r) * J.cw + cx0) * D;
-    for (int i = tid; i < tw * D; i += blockDim.x)
-    {
-      const int c = i / D;
-      out[i] = s_out[(r * kCostTileW + c) * sd + (i - c * D)];
-    }
-  }
-  if (!write_l1)
-    return;
-  // level 1 of the cost pyramid from the tile's costs (cost_distribute,
-  // bpextract.cu:169-198): the existing 2x2 children summed from 0, x
-  // offset outer, y offset inner -- the same additions as k_pyramid
-  const LevelDesc &L1 = J.lv[1];
-  const int x1 = cx0 / 2, y1 = ty, n1 = min(kCostTileW / 2, L1.w - x1);
-  float *out1 = L1.data + ((size_t)y1 * L1.w + x1) * D;
-  for (int i = tid; i < n1 * D; i += blockDim.x)
-  {
-    const int c = i / D, d = i - c * D;
-    float v = 0.0f;
-#pragma unroll
-    for (int ix = 0; ix < 2; ++ix)
-#pragma unroll
-      for (int iy = 0; iy < 2; ++iy)
-        if (2 * c + ix < tw && iy < th)
-          v += s_out[(iy * kCostTileW + 2 * c + ix) * sd + d];
-    out1[i] = v;
+    const int c = i / D;
+    out[i] = s_out[c * sd + (i - c * D)];
   }
 }
 
 } // namespace
 
-int cost_blocks(int cw, int ch)
-{
-  return ((ch + 1) / 2) * ((cw + kCostTileW - 1) / kCostTileW);
-}
+int cost_blocks(int cw, int ch) { return ch * ((cw + kCostCells - 1) / kCostCells); }
 
-void launch_cost(const Batch &B, int blocks, int arith, int max_d, cudaStream_t s, int write_l1)
+void launch_cost(const Batch &B, int blocks, int arith, int max_d, cudaStream_t s)
 {
   const size_t sm = sizeof(float) * kCostCells * (max_d + 1);
   if (arith == QM_ARITH_IEEE)
-    k_cost<ArithIeee><<<blocks, kFlatThreads, sm, s>>>(B, write_l1);
+    k_cost<ArithIeee><<<blocks, kFlatThreads, sm, s>>>(B);
   else
-    k_cost<ArithRef><<<blocks, kFlatThreads, sm, s>>>(B, write_l1);
+    k_cost<ArithRef><<<blocks, kFlatThreads, sm, s>>>(B);
 }
 
 } // namespace qm

@@ -48,16 +48,12 @@ int quadtree_blocks(int W, int H, int qt_max);
 // Every launcher takes the batch by value (the kernels receive it as a
 // __grid_constant__ parameter); B.prefix must point at the stage's prefix.
 void launch_quadtree(const Batch &B, int blocks, KParams kp, cudaStream_t s);
-// cells per block of the cost kernel: a tile of kCostTileW cells of two
-// cell rows
-constexpr int kCostTileW = 16;
-constexpr int kCostCells = 2 * kCostTileW;
+// cells per block of the cost kernel (one tile of a cell row)
+constexpr int kCostCells = 32;
 constexpr int kMaxHyp = 128;
 int cost_blocks(int cw, int ch);
-// max_d: largest hypothesis count of the batch (sizes the shared tile);
-// write_l1: also write the level-1 pyramid data (J.lv[1]) of every tile
-void launch_cost(const Batch &B, int blocks, int arith, int max_d, cudaStream_t s,
-                 int write_l1 = 0);
+// max_d: largest hypothesis count of the batch (sizes the shared tile)
+void launch_cost(const Batch &B, int blocks, int arith, int max_d, cudaStream_t s);
 void launch_pyramid(const Batch &B, int blocks, int level, cudaStream_t s);
 // writes the inherited messages of level `level` that its sweeps will read
 // (cells the quadtree test skips; all unswept cells when iters < 2)
