@@ -21,6 +21,11 @@ Prints one JSON line per workload (seeded synthetic ray-cast scenes):
 
 Per-step latencies flush the L2 (a 256 MiB write) before every timed step;
 back-to-back throughput runs use working sets larger than the L2.
+
+Under torchrun (`python -m torch.distributed.run --nproc-per-node N -m
+open_quadtree_mapping_b200.workloads --only uneven16 large1080`) the batch
+workloads place their streams over the N GPUs (sharding.ShardedBatch) and
+report the max over ranks of the step times.
 """
 from __future__ import annotations
 
@@ -87,12 +92,36 @@ class _Timer:
         return e0.elapsed_time(e1) / steps
 
 
+def _dist():
+    """(world, rank, local rank) from the torchrun environment; with more
+    than one process the NCCL group is set up (one process per GPU)."""
+    import os
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        if not dist.is_initialized():
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
 def _batch_workload(name, descs, seqs, layout, params, steps, warm_frames, extra):
+    """One batch workload.  Under torchrun the streams are placed over the
+    ranks (sharding.ShardedBatch, no data crosses ranks) and the step times
+    are the max over ranks; maps/s counts every rank's streams."""
     import torch
 
-    from .depthmap import BatchDepthmap
+    from .sharding import ShardedBatch, max_over_ranks
+    world, rank, local = _dist()
     S = len(descs)
-    batch = BatchDepthmap(descs, params=params)
+    shard = ShardedBatch(descs, rank, world, params=params, device=local)
+    batch = shard.batch
+    layout = [layout[i] for i in shard.mine]
     pinned = {}
     for k, sid in enumerate(layout):
         for i, img in enumerate(seqs[sid][0]):
@@ -127,7 +156,11 @@ def _batch_workload(name, descs, seqs, layout, params, steps, warm_frames, extra
     batch.wait()
     e2e_ms = 1000.0 * (time.perf_counter() - t0) / steps
     prof = {k: round(v[0], 4) for k, v in batch.profile().items()}
-    line = {"workload": name, "streams": S, "maps_per_s": round(S / (ms * 1e-3), 2),
+    ms = max_over_ranks(ms)
+    e2e_ms = max_over_ranks(e2e_ms)
+    lat = [max_over_ranks(x) for x in lat]
+    line = {"workload": name, "streams": S, "gpus": world,
+            "maps_per_s": round(S / (ms * 1e-3), 2),
             "kernel_ms_eager": prof,
             "ms_per_step": round(ms, 4),
             "step_latency_ms": {"p50": round(_pct(lat, 50), 4), "p99": round(_pct(lat, 99), 4),
@@ -310,14 +343,29 @@ WORKLOADS = {"video720": video720, "uneven16": uneven16, "large1080": large1080,
              "diff8": diff8, "semidense32": semidense32}
 
 
+SHARDED = ("uneven16", "large1080")
+
+
 def main():
+    """Under torchrun (one process per GPU) only the batch workloads run,
+    their streams placed over the GPUs; rank 0 prints."""
+    import os
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", nargs="*", default=list(WORKLOADS))
     ap.add_argument("--steps", type=int, default=20)
     args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
     for name in args.only:
+        if world > 1 and name not in SHARDED:
+            continue
         line = WORKLOADS[name](args.steps)
-        print(json.dumps(line), flush=True)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 if __name__ == "__main__":
