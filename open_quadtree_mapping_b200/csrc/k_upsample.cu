@@ -86,10 +86,13 @@ struct Line
 {
   int rd, ri, cp, img;
   int n, m, mp;
-  float w_close; // weight between samples n - 1 and n (the closing weight)
+  unsigned m_inv; // ceil(2^32 / m): k / m = umulhi(k, m_inv) for 0 <= k < 2^20
+  float w_close;  // weight between samples n - 1 and n (the closing weight)
   __device__ __forceinline__ int pos(int k) const
   {
-    const int l = k / m;
+    // with m_inv = (2^32 + e) / m, 0 <= e < m, umulhi gives floor(k/m + k e /
+    // (m 2^32)), exact while k e < 2^32 (k < 2^20 here, m <= 132)
+    const int l = (int)__umulhi((unsigned)k, m_inv);
     return l * mp + (k - l * m);
   }
 };
@@ -105,6 +108,7 @@ __device__ __forceinline__ Line line_at(int base, int n, float w_close)
   L.n = n;
   L.m = seg_len(n);
   L.mp = seg_pitch(n);
+  L.m_inv = 0xffffffffu / (unsigned)L.m + 1u;
   L.w_close = w_close;
   return L;
 }
@@ -116,11 +120,6 @@ __device__ __forceinline__ float4 ld4(int arr, int p)
 __device__ __forceinline__ void st4(int arr, int p, float4 v)
 {
   *reinterpret_cast<float4 *>(g_smem + arr + 4 * p) = v;
-}
-// the four image bytes of samples k .. k + 3 (k a chunk start)
-__device__ __forceinline__ unsigned ldw(const Line &L, int k)
-{
-  return *reinterpret_cast<const unsigned *>(g_smem + L.img + L.pos(k));
 }
 __device__ __forceinline__ float f4(const float4 &v, int t)
 {
@@ -210,20 +209,29 @@ struct Aff
   float g, hd, hi; // z -> g z + h (two right-hand sides)
 };
 
-// Walks the segment [s, e) chunk by chunk: calls f(k, wl[4], wr[4]) with
-// the weights left and right of samples k .. k + 3.  w_0 = 0, w_n = the
-// closing weight, every other from the table.  The image bytes of the next
-// chunk are fetched before the current chunk is processed.
+// Walks the lane's segment [s, e) chunk by chunk (s = lane * m, element s at
+// position base = lane * mp): calls f(k, wl[4], wr[4]) with the weights left
+// and right of samples k .. k + 3.  w_0 = 0, w_n = the closing weight, every
+// other from the table.  The image bytes of the next chunk are fetched
+// before the current chunk is processed.  A segment that does not end the
+// line holds all m samples, so the sample after it is the next lane's first
+// (position base + mp) and the one before a segment with s > 0 is the
+// previous lane's last (position base - mp + m - 1).
 template <class Fn>
-__device__ __forceinline__ void walk_chunks(const Line &L, int s, int e, Fn &&f)
+__device__ __forceinline__ void walk_chunks(const Line &L, int s, int e, int base, Fn &&f)
 {
   if (s >= e)
     return;
-  unsigned word = ldw(L, s);
-  float w0 = s == 0 ? 0.0f : table_weight((int)(word & 0xffu), g_smem[L.img + L.pos(s - 1)]);
+  const unsigned *wimg = reinterpret_cast<const unsigned *>(g_smem + L.img + base);
+  unsigned word = wimg[0];
+  float w0 =
+      s == 0 ? 0.0f : table_weight((int)(word & 0xffu), g_smem[L.img + base - L.mp + L.m - 1]);
   for (int k = s; k < e; k += 4)
   {
-    const unsigned next = k + 4 < L.n ? ldw(L, k + 4) : 0u;
+    const unsigned next = k + 4 < e     ? wimg[(k + 4 - s) >> 2]
+                          : k + 4 < L.n ? *reinterpret_cast<const unsigned *>(
+                                              g_smem + L.img + base + L.mp)
+                                        : 0u;
     float wl[4], wr[4];
     int I[5];
 #pragma unroll
@@ -255,7 +263,7 @@ __device__ __forceinline__ void solve_line(const Line &L, double lam)
   // entries grow by at most 1 + 2*lambda per element, far inside the double
   // range for segments of <= 128 elements, so no per-step rescaling.
   Mat2 P{1.0, 0.0, 0.0, 1.0};
-  walk_chunks(L, s, e, [&](int, const float(&wl)[4], const float(&wr)[4]) {
+  walk_chunks(L, s, e, base, [&](int, const float(&wl)[4], const float(&wr)[4]) {
 #pragma unroll
     for (int t = 0; t < 4; ++t)
     {
@@ -286,7 +294,7 @@ __device__ __forceinline__ void solve_line(const Line &L, double lam)
   Mat2 Q{1.0, 0.0, 0.0, 1.0};
   double Dprev = 1.0;
   Aff F{1.0f, 0.0f, 0.0f};
-  walk_chunks(L, s, e, [&](int k, const float(&wl)[4], const float(&wr)[4]) {
+  walk_chunks(L, s, e, base, [&](int k, const float(&wl)[4], const float(&wr)[4]) {
     const int p = base + (k - s);
     const float4 rd = ld4(L.rd, p), ri = ld4(L.ri, p);
     float4 inv4;
@@ -321,7 +329,7 @@ __device__ __forceinline__ void solve_line(const Line &L, double lam)
   // -------- forward values of the segment, eliminated super-diagonal
   // c'_k = c_k / den_k, back-substitution composition
   Aff G{1.0f, 0.0f, 0.0f};
-  walk_chunks(L, s, e, [&](int k, const float(&wl)[4], const float(&wr)[4]) {
+  walk_chunks(L, s, e, base, [&](int k, const float(&wl)[4], const float(&wr)[4]) {
     const int p = base + (k - s);
     const float4 inv4 = ld4(L.cp, p);
     float4 rd = ld4(L.rd, p), ri = ld4(L.ri, p), cp4;
@@ -450,34 +458,41 @@ __global__ void __launch_bounds__(kMaxColLines * 32)
   const int x0 = lb * lines;
   const int n = H / 8 * 8;
   const int per_line = line_bytes(max_n);
-  const int total = n * lines;
-  // cooperative stripe load: row k, column x0 + c; a batch of loads per
-  // thread in flight before their shared-memory stores
-  for (int t0 = threadIdx.x; t0 < total; t0 += (int)blockDim.x * kLoadBatch)
+  // cooperative stripe load: thread t owns column x0 + t % lines and rows
+  // t / lines + 32 j (blockDim.x = 32 lines); a batch of loads per thread in
+  // flight before their shared-memory stores
+  const int kt = (int)threadIdx.x / lines, c = (int)threadIdx.x - kt * lines;
+  const int xt = x0 + c;
+  const Line Lt = line_at(kTableBytes + c * per_line, n, 0.0f);
+  if (xt < W)
   {
-    float2 rv[kLoadBatch];
-    uint8_t iv[kLoadBatch];
-#pragma unroll
-    for (int u = 0; u < kLoadBatch; ++u)
+    const float2 *rsrc = J.rowres + (size_t)kt * W + xt;
+    const uint8_t *isrc = J.ref + (size_t)kt * J.ref_pitch + xt;
+    const size_t rstep = (size_t)32 * W, istep = (size_t)32 * J.ref_pitch;
+    for (int k0 = kt; k0 < n; k0 += 32 * kLoadBatch)
     {
-      const int t = t0 + u * (int)blockDim.x;
-      const int k = t / lines, x = x0 + (t - k * lines);
-      const bool in = t < total && x < W;
-      rv[u] = in ? J.rowres[(size_t)k * W + x] : make_float2(0.0f, 0.0f);
-      iv[u] = in ? J.ref[(size_t)k * J.ref_pitch + x] : 0;
-    }
+      float2 rv[kLoadBatch];
+      uint8_t iv[kLoadBatch];
 #pragma unroll
-    for (int u = 0; u < kLoadBatch; ++u)
-    {
-      const int t = t0 + u * (int)blockDim.x;
-      const int k = t / lines, c = t - k * lines;
-      if (t >= total || x0 + c >= W)
-        continue;
-      const Line L = line_at(kTableBytes + c * per_line, n, 0.0f);
-      const int p = L.pos(k);
-      smf(L.rd)[p] = rv[u].x;
-      smf(L.ri)[p] = rv[u].y;
-      g_smem[L.img + p] = iv[u];
+      for (int u = 0; u < kLoadBatch; ++u)
+      {
+        const bool in = k0 + 32 * u < n;
+        rv[u] = in ? rsrc[u * rstep] : make_float2(0.0f, 0.0f);
+        iv[u] = in ? isrc[u * istep] : 0;
+      }
+#pragma unroll
+      for (int u = 0; u < kLoadBatch; ++u)
+      {
+        const int k = k0 + 32 * u;
+        if (k >= n)
+          break;
+        const int p = Lt.pos(k);
+        smf(Lt.rd)[p] = rv[u].x;
+        smf(Lt.ri)[p] = rv[u].y;
+        g_smem[Lt.img + p] = iv[u];
+      }
+      rsrc += kLoadBatch * rstep;
+      isrc += kLoadBatch * istep;
     }
   }
   __syncthreads();
@@ -491,15 +506,14 @@ __global__ void __launch_bounds__(kMaxColLines * 32)
     solve_line(line_at(kTableBytes + warp * per_line, n, w_close), kp.up_lambda);
   }
   __syncthreads();
-  for (int t = threadIdx.x; t < total; t += blockDim.x)
+  if (xt < W)
   {
-    const int k = t / lines, c = t - k * lines;
-    const int xc = x0 + c;
-    if (xc >= W)
-      continue;
-    const Line L = line_at(kTableBytes + c * per_line, n, 0.0f);
-    const int p = L.pos(k);
-    J.dense[(size_t)k * W + xc] = A::div(smf(L.rd)[p], smf(L.ri)[p]);
+    float *dst = J.dense + (size_t)kt * W + xt;
+    for (int k = kt; k < n; k += 32, dst += (size_t)32 * W)
+    {
+      const int p = Lt.pos(k);
+      *dst = A::div(smf(Lt.rd)[p], smf(Lt.ri)[p]);
+    }
   }
 }
 
