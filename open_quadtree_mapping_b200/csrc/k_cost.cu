@@ -199,12 +199,26 @@ __global__ void __launch_bounds__(kFlatThreads, 5)
     }
   }
   __syncthreads();
-  // the tile's cells are consecutive in the [cell][D] layout
+  // the tile's cells are consecutive in the [cell][D] layout.  Element i is
+  // s_out[i + i / D]; i / D = umulhi(i, ceil(2^32 / D)), exact for i < 2^20.
+  // D is a multiple of 16, so when the tile starts on a 16-byte boundary
+  // (always in the engine's arena; a caller's cost buffer may not) four
+  // hypotheses of one cell go out per store.
   float *out = J.lv[0].data + ((size_t)cy * J.cw + cx0) * D;
-  for (int i = tid; i < ncells * D; i += blockDim.x)
+  const unsigned dinv = 0xffffffffu / (unsigned)D + 1u;
+  if ((reinterpret_cast<uintptr_t>(out) & 15u) == 0)
   {
-    const int c = i / D;
-    out[i] = s_out[c * sd + (i - c * D)];
+    for (int i4 = tid; i4 < ncells * D / 4; i4 += blockDim.x)
+    {
+      const int i = 4 * i4;
+      const float *src = s_out + i + (int)__umulhi((unsigned)i, dinv);
+      reinterpret_cast<float4 *>(out)[i4] = make_float4(src[0], src[1], src[2], src[3]);
+    }
+  }
+  else
+  {
+    for (int i = tid; i < ncells * D; i += blockDim.x)
+      out[i] = s_out[i + (int)__umulhi((unsigned)i, dinv)];
   }
 }
 

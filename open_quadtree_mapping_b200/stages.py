@@ -43,9 +43,10 @@ def quadtree(img: torch.Tensor, params: Params = Params()) -> torch.Tensor:
 
 
 def cost_volume(ref: torch.Tensor, levels: torch.Tensor, slots, T_slot_ref, cam,
-                params: Params = Params()) -> torch.Tensor:
+                params: Params = Params(), out: torch.Tensor | None = None) -> torch.Tensor:
     """slots: list of (H, W) uint8 CUDA tensors; T_slot_ref: (F, 12) host
-    floats; cam = (fx, fy, cx, cy).  Returns the (H/4, W/4, D) cost volume."""
+    floats; cam = (fx, fy, cx, cy).  Returns the (H/4, W/4, D) cost volume,
+    written into `out` when given (contiguous float32 of that shape)."""
     _need(ref, torch.uint8, "ref")
     _need(levels, torch.uint8, "levels")
     H, W = ref.shape
@@ -54,7 +55,14 @@ def cost_volume(ref: torch.Tensor, levels: torch.Tensor, slots, T_slot_ref, cam,
         _need(s, torch.uint8, "slot")
     ptrs = (ctypes.c_void_p * F)(*[s.data_ptr() for s in slots])
     T = np.ascontiguousarray(np.asarray(T_slot_ref, dtype=np.float32).reshape(F, 12))
-    cost = torch.empty((H // 4, W // 4, params.num_hyp), dtype=torch.float32, device=ref.device)
+    shape = (H // 4, W // 4, params.num_hyp)
+    if out is None:
+        cost = torch.empty(shape, dtype=torch.float32, device=ref.device)
+    else:
+        _need(out, torch.float32, "out")
+        if tuple(out.shape) != shape:
+            raise ValueError("out must have shape %s" % (shape,))
+        cost = out
     c = _lib.QmCamera(*[float(v) for v in cam])
     pc = _pc(params)
     _lib.check(_lib.lib().qm_cost_volume(_ptr(ref), W, W, H, ctypes.byref(c), _ptr(levels), F,

@@ -206,3 +206,26 @@ def test_invalid_arguments_are_rejected(gpu):
     assert L.qm_bp_extract(ctypes.c_void_p(buf.data_ptr()), 64, 64, ctypes.c_void_p(buf.data_ptr()),
                            ctypes.byref(p), ctypes.c_void_p(buf.data_ptr()), None, None,
                            ctypes.c_void_p(buf.data_ptr()), 16, None) == _lib.QM_ERR_WORKSPACE
+
+
+@pytest.mark.parametrize("arith", [ARITH_IEEE, ARITH_REFERENCE])
+def test_cost_volume_into_unaligned_buffer(arith, gpu):
+    """The cost kernel stores four hypotheses at a time where the output is
+    16-byte aligned and one at a time where it is not; a caller's buffer
+    offset by one float gets the same volume as an aligned one."""
+    from open_quadtree_mapping_b200 import stages
+    kf = keyframe(2, 320, 240, 4)
+    p = Params.for_range(48, 0.5, 50.0, arith=arith)
+    ref = torch.from_numpy(kf.ref).to(gpu)
+    slots = [torch.from_numpy(np.ascontiguousarray(m)).to(gpu) for m in kf.meas]
+    levels = stages.quadtree(ref, p)
+    aligned = stages.cost_volume(ref, levels, slots, kf.T_meas_ref, cam_of(kf), p)
+    shape = tuple(aligned.shape)
+    buf = torch.full((aligned.numel() + 1,), float("nan"), dtype=torch.float32, device=gpu)
+    view = buf[1:].view(shape)
+    assert view.data_ptr() % 16 == 4
+    got = stages.cost_volume(ref, levels, slots, kf.T_meas_ref, cam_of(kf), p, out=view)
+    torch.cuda.synchronize()
+    assert got.data_ptr() == view.data_ptr()
+    assert torch.isnan(buf[0])
+    assert torch.equal(got, aligned)
