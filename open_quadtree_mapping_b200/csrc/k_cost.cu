@@ -33,18 +33,20 @@ namespace qm
 namespace
 {
 
-// floor(c + 0.5) for -0.5 <= c < 2^22 - 0.5, which equals the reference's
-// (int)((double)c + 0.5) there, as HALF the integer n = floor(2c + 1): the
-// sum c + (2^22 + 0.5) lies in [2^22, 2^23), where floats are spaced 0.5
-// apart, so rounding it down gives 2^22 + n/2 exactly, and the bit pattern of
-// that float minus the one of 2^22 is n.  The caller shifts right by one.
-// The returned value is the bit pattern itself; kHalfBias = bits(2^22) / 2 is
-// subtracted (folded into the image offset) after the shift.
-__device__ __forceinline__ unsigned twice_round_bits(float c)
+// floor(c + 0.5) for -0.5 <= c < 2^23 - 0.5, which equals the reference's
+// (int)((double)c + 0.5) there, in one rounded operation: 2^23 + 0.5 is not
+// a float, but it is the exact product 24929 * 336.5 (24929 = 97 * 257,
+// 336.5 = 673 / 2), so a fused multiply-add rounded down evaluates
+// RD(2^23 + 0.5 + c) with a single rounding.  That sum lies in [2^23, 2^24),
+// where floats are spaced 1 apart, so the result is 2^23 + floor(c + 0.5)
+// exactly, and its bit pattern minus kBias = bits(2^23) is the integer.  The
+// returned value is the bit pattern; kBias is subtracted (folded into the
+// image offset) by the caller.
+__device__ __forceinline__ unsigned round_bits(float c)
 {
-  return (unsigned)__float_as_int(__fadd_rd(c, 4194304.5f));
+  return (unsigned)__float_as_int(__fmaf_rd(24929.0f, 336.5f, c));
 }
-constexpr unsigned kHalfBias = 0x4A800000u >> 1;
+constexpr unsigned kBias = 0x4B000000u;
 
 // The 3x3 patch coordinates along one axis.  The reference computes
 // (u + a*i) + b*j for i, j in {-1, 0, 1} (i the patch column, j the row).
@@ -139,7 +141,7 @@ __global__ void __launch_bounds__(kFlatThreads, 5)
   // (int)(u + 0.5) in [2, W-2) exactly when u in [1.5, W-2.5) (both bounds
   // are floats, the comparisons exact; NaN fails)
   const float ulo = 1.5f, uhi = (float)W - 2.5f, vhi = (float)H - 2.5f;
-  const unsigned bias = 0u - kHalfBias * ((unsigned)pitch + 1u);
+  const unsigned bias = 0u - kBias * ((unsigned)pitch + 1u);
   // Thread t evaluates node k = t % n at hypotheses g, g + per, g + 2 per,
   // ... (g = t / n, per = threads per node): consecutive lanes hold
   // neighbouring nodes at one depth, whose projections are neighbours in the
@@ -183,8 +185,8 @@ __global__ void __launch_bounds__(kFlatThreads, 5)
           {
             // offset = floor(py+0.5)*pitch + floor(px+0.5), in 32-bit
             // wrap-around arithmetic (the true offset is below 2^31)
-            const unsigned hx = twice_round_bits(px[t]) >> 1;
-            const unsigned hy = twice_round_bits(py[t]) >> 1;
+            const unsigned hx = round_bits(px[t]);
+            const unsigned hy = round_bits(py[t]);
             const unsigned off = hy * (unsigned)pitch + hx + bias;
             s = __usad(patch[t], (unsigned)__ldg(m + off), s);
           }
