@@ -243,42 +243,73 @@ __device__ __forceinline__ void update_px(const JobDesc &J, int idx, double dep,
   J.seeds_out[idx] = make_float4((float)a_p, (float)b_p, (float)mu_p, (float)s2_p);
 }
 
-// kFuseUpdatePx pixels per thread (one: the update is FP64- and issue-bound,
-// and two per thread measured slower at the lower occupancy): depths and
-// keys first, then the sources,
-// then the source seeds (a dependent load), then the updates
+// A block owns kFlatThreads * kFuseUpdatePx consecutive pixels and walks
+// them in kFuseUpdatePx steps of one pixel per thread.  The pixel chain
+// (key -> source, for an empty pixel through its neighbours' keys -> source
+// seed -> FP64 update) is software-pipelined: while step j's update runs,
+// step j+1's source seed and step j+2's key and depth are already in flight,
+// so the dependent loads overlap the arithmetic instead of stalling it.
+// Every pixel's result depends only on its own inputs and on keys this
+// kernel does not write, so the order changes nothing.
 __global__ void __launch_bounds__(kFlatThreads)
     k_fuse_update(const __grid_constant__ Batch B)
 {
   int lb;
   const JobDesc &J = job_of(B, lb);
   const int npx = J.W * J.H;
-  const int base = lb * (int)blockDim.x * kFuseUpdatePx + (int)threadIdx.x;
+  const int step = (int)blockDim.x;
+  const int base = lb * step * kFuseUpdatePx + (int)threadIdx.x;
   const float inv_w = 1.0f / (float)J.W;
-  float dep[kFuseUpdatePx];
-  unsigned long long key[kFuseUpdatePx];
-#pragma unroll
-  for (int u = 0; u < kFuseUpdatePx; ++u)
+  auto pix = [&](int j) { return base + j * step; };
+  // step j: depth and key (loaded two steps ahead), source and its seed
+  // (one step ahead)
+  float dep0 = 0.0f, dep1 = 0.0f;
+  unsigned long long key1 = kEmpty;
+  int pre0 = 0;
+  float4 src0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   {
-    const int idx = base + u * (int)blockDim.x;
-    dep[u] = idx < npx ? J.dense[idx] : 0.0f;
-    key[u] = idx < npx ? J.zkey[idx] : kEmpty;
+    const int i0 = pix(0), i1 = pix(1);
+    unsigned long long key0 = kEmpty;
+    if (i0 < npx)
+    {
+      dep0 = J.dense[i0];
+      key0 = J.zkey[i0];
+    }
+    if (kFuseUpdatePx > 1 && i1 < npx)
+    {
+      dep1 = J.dense[i1];
+      key1 = J.zkey[i1];
+    }
+    pre0 = i0 < npx ? resolve_source(J, i0, key0, inv_w) : 0;
+    if (pre0 > 0)
+      src0 = J.seeds_in[pre0];
   }
-  int pre[kFuseUpdatePx];
-  float4 src[kFuseUpdatePx];
-#pragma unroll
-  for (int u = 0; u < kFuseUpdatePx; ++u)
+  for (int j = 0; j < kFuseUpdatePx; ++j)
   {
-    const int idx = base + u * (int)blockDim.x;
-    pre[u] = idx < npx ? resolve_source(J, idx, key[u], inv_w) : 0;
-    src[u] = pre[u] > 0 ? J.seeds_in[pre[u]] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  }
-#pragma unroll
-  for (int u = 0; u < kFuseUpdatePx; ++u)
-  {
-    const int idx = base + u * (int)blockDim.x;
-    if (idx < npx)
-      update_px(J, idx, (double)dep[u], pre[u], src[u]);
+    const int i0 = pix(j), i1 = pix(j + 1), i2 = pix(j + 2);
+    if (i0 >= npx)
+      break; // later steps are further out
+    int pre1 = 0;
+    float4 src1 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (j + 1 < kFuseUpdatePx && i1 < npx)
+    {
+      pre1 = resolve_source(J, i1, key1, inv_w);
+      if (pre1 > 0)
+        src1 = J.seeds_in[pre1];
+    }
+    float dep2 = 0.0f;
+    unsigned long long key2 = kEmpty;
+    if (j + 2 < kFuseUpdatePx && i2 < npx)
+    {
+      dep2 = J.dense[i2];
+      key2 = J.zkey[i2];
+    }
+    update_px(J, i0, (double)dep0, pre0, src0);
+    dep0 = dep1;
+    pre0 = pre1;
+    src0 = src1;
+    dep1 = dep2;
+    key1 = key2;
   }
 }
 

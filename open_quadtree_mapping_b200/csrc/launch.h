@@ -89,9 +89,9 @@ void launch_row_solve(const Batch &B, int blocks, KParams kp, int arith, int max
 void launch_col_solve(const Batch &B, int blocks, KParams kp, int arith, int max_h,
                       cudaStream_t s, int lines = kColLines);
 // pixels per thread of the fusion transform and update (their blocks cover
-// kFlatThreads times as many)
+// kFlatThreads times as many; the update walks its pixels as a pipeline)
 constexpr int kFuseTransformPx = 4;
-constexpr int kFuseUpdatePx = 1;
+constexpr int kFuseUpdatePx = 8;
 void launch_fuse_transform(const Batch &B, int blocks, int arith, cudaStream_t s);
 // hole filling + posterior update (reads the z-buffer keys, leaves them set:
 // the next frame's row solve resets them)
