@@ -280,6 +280,79 @@ __device__ __forceinline__ float msg_load(const float *p)
     return *p;
 }
 
+// The update of one cell (bp, bpextract.cu:200-312) from its data term and
+// its four incoming messages (zeros, and has_* false, where the level ends),
+// every lane of the warp taking part (groups without a cell pass zeros):
+// for each outgoing direction, emit(dir, m, mean) receives the group's NV
+// values m[k] (hypothesis gl + LPC k) and the mean the message subtracts, so
+// the message is m[k] - mean.
+template <int D, int ARITH, class Emit>
+__device__ __forceinline__ void cell_update(const float (&dat)[HypLayout<D>::NV],
+                                            const float (&fu)[HypLayout<D>::NV],
+                                            const float (&fd)[HypLayout<D>::NV],
+                                            const float (&fl)[HypLayout<D>::NV],
+                                            const float (&fr)[HypLayout<D>::NV], bool has_u,
+                                            bool has_d, bool has_l, bool has_r, const KParams &kp,
+                                            int gl, Emit &&emit)
+{
+  using HL = HypLayout<D>;
+  constexpr int NV = HL::NV, LPC = HL::LPC;
+  const float P1 = kp.P1, P2 = kp.P2;
+  // h of every direction: the data term plus the three other incoming
+  // messages, in the reference's order (up, down, left, right skipped as
+  // named by the direction); computed up front so the raw inputs die early
+  float hall[4][NV];
+#pragma unroll
+  for (int dir = 0; dir < 4; ++dir)
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+    {
+      float v = dat[k];
+      if (dir != kUp && has_u)
+        v += fu[k];
+      if (dir != kDown && has_d)
+        v += fd[k];
+      if (dir != kLeft && has_l)
+        v += fl[k];
+      if (dir != kRight && has_r)
+        v += fr[k];
+      hall[dir][k] = v;
+    }
+#pragma unroll
+  for (int dir = 0; dir < 4; ++dir)
+  {
+    const float(&hv)[NV] = hall[dir];
+    float lmin = FLT_MAX;
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+      lmin = fminf(lmin, hv[k]);
+    const float hmin = group_min<LPC>(lmin);
+    float m[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+    {
+      const int d = gl + LPC * k;
+      // h(d-1): the previous lane's slot k, or for group lane 0 the group's
+      // last lane's slot k-1; h(d+1): the next lane's slot k, or for the last
+      // lane group lane 0's slot k+1.  One shuffle each, the source lane
+      // choosing which register it offers.
+      const float up_src = (gl == LPC - 1 && k > 0) ? hv[k > 0 ? k - 1 : 0] : hv[k];
+      const float dn_src = (gl == 0 && k + 1 < NV) ? hv[k + 1 < NV ? k + 1 : k] : hv[k];
+      const float prev = __shfl_sync(0xffffffffu, up_src, (gl + LPC - 1) & (LPC - 1), LPC);
+      const float next = __shfl_sync(0xffffffffu, dn_src, (gl + 1) & (LPC - 1), LPC);
+      float mv = hv[k];
+      if (d > 0)
+        mv = fminf(mv, prev + P1);
+      if (d < D - 1)
+        mv = fminf(mv, next + P1);
+      m[k] = fminf(mv, hmin + P2);
+    }
+    const float sum = tree_sum<D>(m);
+    const float mean = mean_of<D, ARITH>(sum);
+    emit(dir, m, mean);
+  }
+}
+
 // One warp's lane groups of half-sweep `parity` at `level`: items item0 ..
 // item0 + G - 1 of the colour's cells (item = y * ceil(w / 2) + x / 2).
 template <int D, int ARITH, bool L2_ONLY>
@@ -360,66 +433,16 @@ __device__ __forceinline__ void sweep_warp(const JobDesc &J, int level, int pari
     fl[k] = (ld && has_l) ? msg_load<L2_ONLY>(src_l + d) : 0.0f;
     fr[k] = (ld && has_r) ? msg_load<L2_ONLY>(src_r + d) : 0.0f;
   }
-  const float P1 = kp.P1, P2 = kp.P2;
-  // h of every direction: the data term plus the three other incoming
-  // messages, in the reference's order (up, down, left, right skipped as
-  // named by the direction); computed up front so the raw inputs die early
-  float hall[4][NV];
+  cell_update<D, ARITH>(dat, fu, fd, fl, fr, has_u, has_d, has_l, has_r, kp, gl,
+                        [&](int dir, const float(&m)[NV], float mean) {
+                          if (act)
+                          {
+                            float *out = L.msg[dir] + c * D;
 #pragma unroll
-  for (int dir = 0; dir < 4; ++dir)
-#pragma unroll
-    for (int k = 0; k < NV; ++k)
-    {
-      float v = dat[k];
-      if (dir != kUp && has_u)
-        v += fu[k];
-      if (dir != kDown && has_d)
-        v += fd[k];
-      if (dir != kLeft && has_l)
-        v += fl[k];
-      if (dir != kRight && has_r)
-        v += fr[k];
-      hall[dir][k] = v;
-    }
-#pragma unroll
-  for (int dir = 0; dir < 4; ++dir)
-  {
-    const float(&hv)[NV] = hall[dir];
-    float lmin = FLT_MAX;
-#pragma unroll
-    for (int k = 0; k < NV; ++k)
-      lmin = fminf(lmin, hv[k]);
-    const float hmin = group_min<LPC>(lmin);
-    float m[NV];
-#pragma unroll
-    for (int k = 0; k < NV; ++k)
-    {
-      const int d = gl + LPC * k;
-      // h(d-1): the previous lane's slot k, or for group lane 0 the group's
-      // last lane's slot k-1; h(d+1): the next lane's slot k, or for the last
-      // lane group lane 0's slot k+1.  One shuffle each, the source lane
-      // choosing which register it offers.
-      const float up_src = (gl == LPC - 1 && k > 0) ? hv[k > 0 ? k - 1 : 0] : hv[k];
-      const float dn_src = (gl == 0 && k + 1 < NV) ? hv[k + 1 < NV ? k + 1 : k] : hv[k];
-      const float prev = __shfl_sync(0xffffffffu, up_src, (gl + LPC - 1) & (LPC - 1), LPC);
-      const float next = __shfl_sync(0xffffffffu, dn_src, (gl + 1) & (LPC - 1), LPC);
-      float mv = hv[k];
-      if (d > 0)
-        mv = fminf(mv, prev + P1);
-      if (d < D - 1)
-        mv = fminf(mv, next + P1);
-      m[k] = fminf(mv, hmin + P2);
-    }
-    const float sum = tree_sum<D>(m);
-    const float mean = mean_of<D, ARITH>(sum);
-    if (act)
-    {
-      float *out = L.msg[dir] + c * D;
-#pragma unroll
-      for (int k = 0; k < NV; ++k)
-        out[gl + LPC * k] = m[k] - mean;
-    }
-  }
+                            for (int k = 0; k < NV; ++k)
+                              out[gl + LPC * k] = m[k] - mean;
+                          }
+                        });
 }
 
 template <int D, int ARITH>
