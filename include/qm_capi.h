@@ -229,12 +229,15 @@ int qm_batch_set_stagger(qm_batch *b, int enable);
 typedef struct qm_tune
 {
   int sweep_warps, extract_warps, row_warps, col_lines;
+  /* resident blocks per SM the cost kernel is built for (3, 4 or 5: the
+   * register budget per thread, 80, 64 or 48) */
+  int cost_blocks;
 } qm_tune;
 /* 1 = autotune (the default): every set of streams that runs together times
  * three candidate shapes per kernel family on its first run (seven eager
  * runs that change no result) and keeps the fastest; 0 = the fixed shapes
- * (the defaults 8, 8, 2, 4 unless qm_batch_set_tune set others).  Results do
- * not depend on the shapes. */
+ * (the defaults 8, 8, 2, 4, 5 unless qm_batch_set_tune set others).  Results
+ * do not depend on the shapes. */
 int qm_batch_set_autotune(qm_batch *b, int enable);
 /* Fixes the shapes and turns autotune off.  QM_ERR_INVALID_ARG for a value
  * outside the sets above or a line-solver block whose lines exceed the

@@ -908,6 +908,7 @@ int qm_batch_set_tune(qm_batch *b, const qm_tune *t)
     u.extract_warps = t->extract_warps;
     u.row_warps = t->row_warps;
     u.col_lines = t->col_lines;
+    u.cost_blocks = t->cost_blocks;
     b->set->engine().set_tune(u);
   });
 }
@@ -921,6 +922,7 @@ int qm_batch_get_tune(qm_batch *b, qm_tune *t)
     t->extract_warps = u.extract_warps;
     t->row_warps = u.row_warps;
     t->col_lines = u.col_lines;
+    t->cost_blocks = u.cost_blocks;
   });
 }
 

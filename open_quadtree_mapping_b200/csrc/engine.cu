@@ -188,7 +188,8 @@ int enqueue_range(const Batch &B, const StageTable &T, const qm_params &p, size_
   };
   all(kQuadtree, st.qt(), [&](const Batch &b, int g) { launch_quadtree(b, g, kp, s); });
   const int max_d = T.dvals.empty() ? 0 : T.dvals.back();
-  all(kCost, st.cost(), [&](const Batch &b, int g) { launch_cost(b, g, ar, max_d, s); });
+  all(kCost, st.cost(),
+      [&](const Batch &b, int g) { launch_cost(b, g, ar, max_d, s, T.tune.cost_blocks); });
   for (int l = 1; l < L; ++l)
     all(kPyramid, st.pyr(l), [&](const Batch &b, int g) { launch_pyramid(b, g, l, s); });
   // BP, coarse to fine.  The top levels lc..L-1 whose cells are few (and
@@ -486,6 +487,8 @@ std::string validate(const Tune &t, int max_w, int max_h)
     return "BP warps per block must be 4, 8 or 16";
   if (!one_of(t.row_warps, 1, 2, 4) || !one_of(t.col_lines, 2, 4, 8))
     return "row-solve rows per block must be 1, 2 or 4 and column-solve lines 2, 4 or 8";
+  if (!one_of(t.cost_blocks, 3, 4, 5))
+    return "cost-kernel blocks per SM must be 3, 4 or 5";
   if (row_solve_smem(max_w, t.row_warps) > (size_t)kMaxBlockSmem ||
       col_solve_smem(max_h, t.col_lines) > (size_t)kMaxBlockSmem)
     return "line-solver block exceeds the shared memory of a block at this image size";
@@ -743,8 +746,10 @@ Plan &Engine::plan_for(const std::vector<int> &active)
 static Tune candidate(int c, int max_w, int max_h)
 {
   static const int kWarps[3] = {4, 8, 16}, kRows[3] = {1, 2, 4}, kCols[3] = {2, 4, 8};
+  static const int kCostB[3] = {4, kCostBlocks, 3};
   Tune t;
   t.sweep_warps = t.extract_warps = kWarps[c];
+  t.cost_blocks = kCostB[c];
   if (row_solve_smem(max_w, kRows[c]) <= (size_t)kMaxBlockSmem)
     t.row_warps = kRows[c];
   if (col_solve_smem(max_h, kCols[c]) <= (size_t)kMaxBlockSmem)
@@ -754,7 +759,7 @@ static Tune candidate(int c, int max_w, int max_h)
 
 void Engine::tune_plan(Plan &pl)
 {
-  // The candidates of the four families are timed side by side: run c uses
+  // The candidates of the five families are timed side by side: run c uses
   // candidate c of each, and every family keeps its fastest candidate by the
   // summed device time of its launches.  Runs are eager, with an event pair
   // around every launch; the first run warms the caches and is not counted,
@@ -767,8 +772,8 @@ void Engine::tune_plan(Plan &pl)
     cand[c] = build_table(pl.active, candidate(c, T0.max_w, T0.max_h));
   const Batch B = upload((int)pl.active.size(), stream_);
   const Stages st{params_.bp_levels};
-  const int fam_kind[4] = {kSweep, kExtract, kRowSolve, kColSolve};
-  float best[3][4];
+  const int fam_kind[5] = {kSweep, kExtract, kRowSolve, kColSolve, kCost};
+  float best[3][5];
   for (auto &r : best)
     for (float &v : r)
       v = INFINITY;
@@ -802,11 +807,11 @@ void Engine::tune_plan(Plan &pl)
       cudaEventDestroy(m.e1);
     }
     if (r > 0)
-      for (int f = 0; f < 4; ++f)
+      for (int f = 0; f < 5; ++f)
         best[c][f] = std::min(best[c][f], ms[fam_kind[f]]);
   }
-  int pick[4];
-  for (int f = 0; f < 4; ++f)
+  int pick[5];
+  for (int f = 0; f < 5; ++f)
   {
     pick[f] = 1;
     for (int c = 0; c < 3; ++c)
@@ -818,6 +823,7 @@ void Engine::tune_plan(Plan &pl)
   t.extract_warps = cand[pick[1]]->table.tune.extract_warps;
   t.row_warps = cand[pick[2]]->table.tune.row_warps;
   t.col_lines = cand[pick[3]]->table.tune.col_lines;
+  t.cost_blocks = cand[pick[4]]->table.tune.cost_blocks;
   pl.drop_graphs();
   pl.tb = build_table(pl.active, t);
   pl.tuned = true;

@@ -65,12 +65,14 @@ __device__ __forceinline__ void patch_axis(float u, float a, float b, float (&c)
   }
 }
 
-// At most 48 registers (5 blocks of 256 threads per SM): the kernel is
-// issue-bound and gains more from resident warps than it loses to a few
-// spilled values (measured on a B200, 1920x1080 / 128 hypotheses / 20 slots:
-// 2.29 ms per 2 streams at 5 blocks, 2.65 ms at 60 registers).
-template <class A>
-__global__ void __launch_bounds__(kFlatThreads, 5)
+// MINB resident blocks of 256 threads per SM (at most 48, 64 or 80
+// registers for 5, 4 or 3): more resident warps against fewer spilled
+// values.  Which wins depends on the workload (measured on a B200: 32 x
+// 752x480 with 64 hypotheses and 5 slots 0.969 ms at 4 blocks against 1.022
+// at 5; 2 x 1920x1080 with 128 hypotheses and 20 slots 3.456 ms per run at
+// 4 against 3.377 at 5), so the engine's autotuner picks it per stream set.
+template <class A, int MINB>
+__global__ void __launch_bounds__(kFlatThreads, MINB)
     k_cost(const __grid_constant__ Batch B)
 {
   // costs of the tile, [kCostCells][D + 1] (the padding keeps lanes that
@@ -228,13 +230,28 @@ __global__ void __launch_bounds__(kFlatThreads, 5)
 
 int cost_blocks(int cw, int ch) { return ch * ((cw + kCostCells - 1) / kCostCells); }
 
-void launch_cost(const Batch &B, int blocks, int arith, int max_d, cudaStream_t s)
+namespace
+{
+template <int MINB>
+void cost_minb(const Batch &B, int blocks, int arith, size_t sm, cudaStream_t s)
+{
+  if (arith == QM_ARITH_IEEE)
+    k_cost<ArithIeee, MINB><<<blocks, kFlatThreads, sm, s>>>(B);
+  else
+    k_cost<ArithRef, MINB><<<blocks, kFlatThreads, sm, s>>>(B);
+}
+} // namespace
+
+void launch_cost(const Batch &B, int blocks, int arith, int max_d, cudaStream_t s,
+                 int blocks_per_sm)
 {
   const size_t sm = sizeof(float) * kCostCells * (max_d + 1);
-  if (arith == QM_ARITH_IEEE)
-    k_cost<ArithIeee><<<blocks, kFlatThreads, sm, s>>>(B);
+  if (blocks_per_sm == 3)
+    cost_minb<3>(B, blocks, arith, sm, s);
+  else if (blocks_per_sm == 4)
+    cost_minb<4>(B, blocks, arith, sm, s);
   else
-    k_cost<ArithRef><<<blocks, kFlatThreads, sm, s>>>(B);
+    cost_minb<5>(B, blocks, arith, sm, s);
 }
 
 } // namespace qm

@@ -23,6 +23,8 @@ constexpr int kRowWarps = 2;
 constexpr int kColLines = 4;
 constexpr int kMaxRowWarps = 4;
 constexpr int kMaxColLines = 8;
+// cost kernel: resident blocks of 256 threads per SM it is compiled for
+constexpr int kCostBlocks = 5;
 // longest lines the solvers' shared memory holds
 constexpr int kMaxRowLen = 4096;
 constexpr int kMaxColLen = 2048;
@@ -39,6 +41,7 @@ struct Tune
   int extract_warps = kCellWarps; // warps per block of the extraction
   int row_warps = kRowWarps;      // rows per block of the row solve
   int col_lines = kColLines;      // columns per block of the column solve
+  int cost_blocks = kCostBlocks;  // resident cost-kernel blocks per SM (3, 4 or 5)
 };
 void prepare_upsample_kernels();
 
@@ -52,8 +55,10 @@ void launch_quadtree(const Batch &B, int blocks, KParams kp, cudaStream_t s);
 constexpr int kCostCells = 32;
 constexpr int kMaxHyp = 128;
 int cost_blocks(int cw, int ch);
-// max_d: largest hypothesis count of the batch (sizes the shared tile)
-void launch_cost(const Batch &B, int blocks, int arith, int max_d, cudaStream_t s);
+// max_d: largest hypothesis count of the batch (sizes the shared tile);
+// blocks_per_sm: 3, 4 or 5, the instance's register budget
+void launch_cost(const Batch &B, int blocks, int arith, int max_d, cudaStream_t s,
+                 int blocks_per_sm = kCostBlocks);
 void launch_pyramid(const Batch &B, int blocks, int level, cudaStream_t s);
 // writes the inherited messages of level `level` that its sweeps will read
 // (cells the quadtree test skips; all unswept cells when iters < 2)

@@ -304,20 +304,21 @@ class BatchDepthmap:
         """Branch i + 1 starts after branch i's cost volume (default off)."""
         _lib.check(_lib.lib().qm_batch_set_stagger(self._h, 1 if on else 0))
 
-    TUNE_FIELDS = ("sweep_warps", "extract_warps", "row_warps", "col_lines")
+    TUNE_FIELDS = ("sweep_warps", "extract_warps", "row_warps", "col_lines", "cost_blocks")
 
     def set_autotune(self, on: bool) -> None:
         """Time candidate launch shapes per active stream set (default on)."""
         _lib.check(_lib.lib().qm_batch_set_autotune(self._h, 1 if on else 0))
 
-    def set_tune(self, sweep_warps=8, extract_warps=8, row_warps=2, col_lines=4) -> None:
+    def set_tune(self, sweep_warps=8, extract_warps=8, row_warps=2, col_lines=4,
+                 cost_blocks=5) -> None:
         """Fix the launch shapes (turns autotune off)."""
-        t = (ctypes.c_int * 4)(sweep_warps, extract_warps, row_warps, col_lines)
+        t = (ctypes.c_int * 5)(sweep_warps, extract_warps, row_warps, col_lines, cost_blocks)
         _lib.check(_lib.lib().qm_batch_set_tune(self._h, t))
 
     def get_tune(self) -> dict:
         """Launch shapes of the last run."""
-        t = (ctypes.c_int * 4)()
+        t = (ctypes.c_int * 5)()
         _lib.check(_lib.lib().qm_batch_get_tune(self._h, t))
         return dict(zip(self.TUNE_FIELDS, list(t)))
 

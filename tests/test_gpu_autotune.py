@@ -2,8 +2,9 @@
 qm_batch_set_tune / qm_batch_get_tune), through the C-ABI.
 
 The BP half-sweep, extraction, row-solve and column-solve kernels take their
-block shape at launch; whatever shapes are chosen, every fused depth and
-debug map is bit-identical."""
+block shape at launch, the cost kernel its register budget (resident blocks
+per SM); whatever shapes are chosen, every fused depth and debug map is
+bit-identical."""
 import numpy as np
 import pytest
 
@@ -14,9 +15,9 @@ pytestmark = pytest.mark.gpu
 
 SHAPES = [(160, 128, 64, 5), (192, 144, 48, 3), (128, 96, 96, 7), (160, 120, 32, 2)]
 FIXED = [
-    dict(sweep_warps=4, extract_warps=16, row_warps=1, col_lines=8),
-    dict(sweep_warps=16, extract_warps=4, row_warps=4, col_lines=2),
-    dict(sweep_warps=8, extract_warps=8, row_warps=2, col_lines=4),
+    dict(sweep_warps=4, extract_warps=16, row_warps=1, col_lines=8, cost_blocks=3),
+    dict(sweep_warps=16, extract_warps=4, row_warps=4, col_lines=2, cost_blocks=4),
+    dict(sweep_warps=8, extract_warps=8, row_warps=2, col_lines=4, cost_blocks=5),
 ]
 
 
@@ -53,6 +54,7 @@ def test_results_do_not_depend_on_launch_shapes(gpu):
     t = tuned.get_tune()
     assert t["sweep_warps"] in (4, 8, 16) and t["extract_warps"] in (4, 8, 16)
     assert t["row_warps"] in (1, 2, 4) and t["col_lines"] in (2, 4, 8)
+    assert t["cost_blocks"] in (3, 4, 5)
     for b, want in zip(fixed, FIXED):
         assert b.get_tune() == want
     # switching back to autotune re-plans and still gives the same maps
@@ -68,7 +70,7 @@ def test_invalid_launch_shapes_are_rejected(gpu):
     from open_quadtree_mapping_b200.depthmap import BatchDepthmap
     b = BatchDepthmap(_descs()[:1], params=Params.for_range(64, 0.5, 50.0))
     for bad in (dict(sweep_warps=5), dict(extract_warps=32), dict(row_warps=3),
-                dict(col_lines=16)):
+                dict(col_lines=16), dict(cost_blocks=6), dict(cost_blocks=2)):
         with pytest.raises(_lib.QmError):
             b.set_tune(**bad)
     # lines of 4096 samples (the longest rows): at 13 bytes of shared memory
