@@ -230,7 +230,8 @@ typedef struct qm_tune
 {
   int sweep_warps, extract_warps, row_warps, col_lines;
   /* resident blocks per SM the cost kernel is built for (3, 4 or 5: the
-   * register budget per thread, 80, 64 or 48) */
+   * register budget per thread, 80, 64 or 48; 0 in qm_batch_set_tune = the
+   * default 5) */
   int cost_blocks;
 } qm_tune;
 /* 1 = autotune (the default): every set of streams that runs together times

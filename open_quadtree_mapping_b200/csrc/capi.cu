@@ -908,7 +908,8 @@ int qm_batch_set_tune(qm_batch *b, const qm_tune *t)
     u.extract_warps = t->extract_warps;
     u.row_warps = t->row_warps;
     u.col_lines = t->col_lines;
-    u.cost_blocks = t->cost_blocks;
+    // 0 (a qm_tune initialised with the four block shapes only): the default
+    u.cost_blocks = t->cost_blocks == 0 ? qm::kCostBlocks : t->cost_blocks;
     b->set->engine().set_tune(u);
   });
 }

@@ -79,3 +79,6 @@ def test_invalid_launch_shapes_are_rejected(gpu):
                                num_hyp=32, num_slots=1)], params=Params.for_range(32, 0.5, 50.0))
     wide.set_tune(row_warps=4)
     wide.set_tune(row_warps=2)
+    # a cost budget of 0 (a qm_tune filled with the four block shapes only)
+    # selects the default instead of being rejected
+    wide.set_tune(cost_blocks=0)
