@@ -67,10 +67,11 @@ __device__ __forceinline__ void patch_axis(float u, float a, float b, float (&c)
 
 // MINB resident blocks of 256 threads per SM (at most 48, 64 or 80
 // registers for 5, 4 or 3): more resident warps against fewer spilled
-// values.  Which wins depends on the workload (measured on a B200: 32 x
+// values.  The balance depends on the hypothesis and slot counts, so the
+// engine's autotuner picks it per stream set (measured on a B200: 32 x
 // 752x480 with 64 hypotheses and 5 slots 0.969 ms at 4 blocks against 1.022
-// at 5; 2 x 1920x1080 with 128 hypotheses and 20 slots 3.456 ms per run at
-// 4 against 3.377 at 5), so the engine's autotuner picks it per stream set.
+// at 5; at 8 x 1920x1080 with 128 hypotheses and 20 slots the tuner also
+// picks 4, 8.13 ms against 8.90 with 5).
 template <class A, int MINB>
 __global__ void __launch_bounds__(kFlatThreads, MINB)
     k_cost(const __grid_constant__ Batch B)
