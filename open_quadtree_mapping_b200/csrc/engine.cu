@@ -234,18 +234,25 @@ int enqueue_range(const Batch &B, const StageTable &T, const qm_params &p, size_
       }
       if (l < lc && in(st.sweep(l)))
       {
-        const Batch b = at(st.sweep(l), j0, j1, grid);
+        // consecutive half-sweeps walk the cells in opposite orders, so each
+        // starts on the messages its predecessor wrote last (still in L2)
+        Batch b = at(st.sweep(l), j0, j1, grid);
         if (grid > 0)
           for (int it = 0; it < p.bp_iters[l]; ++it)
+          {
+            b.rev = it & 1;
             for (int d : T.dvals)
               launch(kSweep, [&] {
                 launch_bp_sweep(b, grid, d, l, it, kp, ar, s, T.tune.sweep_warps,
                                 fold && in(st.inherit(l)) ? 1 : 0);
               });
+          }
       }
       if (l == 0 && in(st.extract()))
       {
-        const Batch b = at(st.extract(), j0, j1, grid);
+        // against the order of the level's last half-sweep (see above)
+        Batch b = at(st.extract(), j0, j1, grid);
+        b.rev = (l < lc && p.bp_iters[0] > 0) ? 1 - ((p.bp_iters[0] - 1) & 1) : 0;
         if (grid > 0)
           for (int d : T.dvals)
             launch(kExtract, [&] { launch_extract(b, grid, d, ar, s, T.tune.extract_warps); });

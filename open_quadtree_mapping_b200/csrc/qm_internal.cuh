@@ -97,6 +97,7 @@ struct Batch
   int njobs;
   int block0;  // global block index of this launch's first block (job groups)
   int uniform; // > 0: every job has this many blocks (job = block / uniform)
+  int rev;     // 1: blocks take their work in reverse order (last block first)
   const uint8_t *const *slot_ptr; // per slot, device image (null: `slots`)
   const float *slot_T;            // per slot, 12 floats T_slot<-ref
   const int *slot_w;              // per slot, multiplicity
@@ -131,7 +132,8 @@ __device__ __forceinline__ int find_job(const int *__restrict__ prefix, int njob
 // cover a contiguous group of jobs only: its blocks then start at block0.
 __device__ __forceinline__ const JobDesc &job_of(const Batch &B, int &local_block)
 {
-  const int block = (int)blockIdx.x + B.block0;
+  const int block =
+      (B.rev ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x) + B.block0;
   if (B.jobs == nullptr)
   {
     local_block = block;
