@@ -221,11 +221,12 @@ int qm_batch_set_coarse_bp(qm_batch *b, int max_cells);
  * measured faster) = all branches start together.  Results do not depend
  * on it. */
 int qm_batch_set_stagger(qm_batch *b, int enable);
-/* Launch shapes of the BP and line-solver kernels: warps per block of the
- * BP half-sweeps and of the extraction (4, 8 or 16), rows per block of the
- * row solve (1, 2 or 4) and columns per block of the column solve (2, 4 or
- * 8).  The reference fixes its block shapes at compile time
- * (bp_extract.cu, depth_upsample.cu launches); no counterpart. */
+/* Launch shapes of the BP, line-solver and cost kernels: warps per block of
+ * the BP half-sweeps and of the extraction (4, 8 or 16), rows per block of
+ * the row solve (1, 2 or 4), columns per block of the column solve (2, 4 or
+ * 8) and the cost kernel's register budget.  The reference fixes its block
+ * shapes at compile time (bpextract.cu, depth_upsample.cu,
+ * seed_matrix.cu launches); no counterpart. */
 typedef struct qm_tune
 {
   int sweep_warps, extract_warps, row_warps, col_lines;

@@ -47,6 +47,24 @@ def test_default_params_match_reference_constants(L):
     assert ctypes.sizeof(QmParamsC) == ctypes.sizeof(p)
 
 
+def test_tune_fields_match_header():
+    """The Python binding passes qm_tune as a plain int array in field order:
+    the header's struct must list exactly those int fields, in that order."""
+    import re
+    from open_quadtree_mapping_b200.depthmap import BatchDepthmap
+    text = open(_lib.HEADER).read()
+    body = re.search(r"typedef struct qm_tune\s*\{(.*?)\}\s*qm_tune;", text, re.S).group(1)
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    fields = []
+    for decl in body.split(";"):
+        decl = decl.strip()
+        if not decl:
+            continue
+        assert decl.startswith("int "), decl
+        fields += [f.strip() for f in decl[4:].split(",")]
+    assert tuple(fields) == BatchDepthmap.TUNE_FIELDS
+
+
 def test_invalid_arguments_without_gpu(L):
     p = _lib.default_params()
     assert L.qm_quadtree(None, 0, 2, 2, ctypes.byref(p), None, None) == _lib.QM_ERR_INVALID_ARG
