@@ -103,6 +103,44 @@ def test_no_alloc_calls_leave_free_device_memory_unchanged(gpu):
     np.testing.assert_allclose(got, want, rtol=RTOL, atol=0)
 
 
+def test_no_alloc_call_captured_in_graph_after_setup(gpu):
+    """The documented set-up order: one eager call on the device first, then
+    a later call can be captured into a CUDA graph (global capture mode, so
+    any call that is unsafe during capture would fail the capture).  The
+    replayed graph, on new inputs copied into the captured buffers, gives
+    the eager result for those inputs."""
+    dev = gpu
+    params = Params(arith=ARITH_REFERENCE)
+    W, H = 752, 480
+    img_h, sparse_h = _case(W, H, 11)
+    img = torch.from_numpy(img_h).to(dev)
+    sparse = torch.from_numpy(sparse_h).to(dev)
+    dense = torch.full((H, W), float("nan"), dtype=torch.float32, device=dev)
+    side = torch.cuda.Stream(device=dev)
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        st = ctypes.c_void_p(side.cuda_stream)
+        assert _no_alloc(sparse, img, params, dense, st) == 0, _lib.lib().qm_last_error()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        cap = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        rc = _no_alloc(sparse, img, params, dense, cap)
+    assert rc == 0, _lib.lib().qm_last_error()
+    img2_h, sparse2_h = _case(W, H, 12)
+    img.copy_(torch.from_numpy(img2_h))
+    sparse.copy_(torch.from_numpy(sparse2_h))
+    dense.fill_(float("nan"))
+    g.replay()
+    torch.cuda.synchronize()
+    got = dense.cpu().numpy()
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    want = _with_workspace(sparse, img, params, stream).cpu().numpy()
+    assert np.isfinite(got).all()
+    np.testing.assert_allclose(got, want, rtol=RTOL, atol=0)
+    del g
+
+
 def test_no_alloc_rejects_oversize_and_bad_shapes(gpu):
     dev = gpu
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
