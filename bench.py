@@ -223,9 +223,10 @@ def algorithmic_bytes(levels_list, params):
 
 def dram_traffic(kind, streams):
     """DRAM bytes (read + write) per launch of kernel kind `kind` from the
-    committed ncu capture of this workload (profiles/), scaled by the stream
-    count when the bench runs a different one.  (None, reason) if absent."""
-    path = os.path.join(ROOT, "profiles", "dram_traffic_752x480x64_32streams.json")
+    committed ncu capture (profiles/: a few launches per BP level of the
+    4-stream case of this workload), scaled by the stream count the bench
+    runs.  (None, reason) if absent."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic_bp_752x480x64_4streams.json")
     try:
         with open(path) as f:
             cap = json.load(f)
